@@ -1,0 +1,421 @@
+"""Python host mirror of the B200 pseudospectral step (ctypes over the C ABI).
+
+The operator surface follows the reference solver (mfkiwl/gnss-1):
+``forward_transform`` / ``inverse_transform`` (fftfuncs.cu:288-359),
+``de_alias``, ``vorticity``, ``gradient``, ``divergence``, ``make_rhs``,
+``timestep``, ``update``, ``cross_product``, ``dot_product``,
+``colloid_advection`` and ``solver_ps`` (solver.cu), and the spectral
+statistics of statistics.cu:1494-1845.  Buffers are device memory in the
+reference layouts (spectral complex [ny][nx][nz2], physical real padded
+[nx][ny][2*nz2], one buffer per field, transforms in place).
+
+Arguments may be torch CUDA tensors or raw device pointers (ints).  Every call
+raises :class:`GnssError` on a non-zero status.  The shared library must be
+built (``python gnss-1_b200/build.py``); importing this module on a machine
+where it is missing raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from pathlib import Path
+from typing import Iterable, Sequence
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libgnss_b200.so"
+
+GNSS_OK = 0
+GNSS_SCHEME_CNAB2 = 0
+GNSS_SCHEME_RK3IF = 1
+GNSS_FP64 = 0
+GNSS_FP32 = 1
+GNSS_NSTATS = 7
+STAT_NAMES = ("ke", "vrms2", "eps", "chi_s", "chi_c", "var_s", "var_c")
+SUPPORTED_SIZES = (8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512)
+
+
+class GnssError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str = ""):
+        super().__init__(f"{what}: status {status}" + (f" ({detail})" if detail else ""))
+        self.status = status
+
+
+class GnssConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("re", ctypes.c_double), ("sc", ctypes.c_double), ("sc_c", ctypes.c_double),
+        ("alpha", ctypes.c_double), ("dt", ctypes.c_double),
+        ("alias_filter", ctypes.c_double), ("nu_stats", ctypes.c_double),
+        ("n_scalars", ctypes.c_int), ("scheme", ctypes.c_int), ("precision", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class GnssFields(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p),
+                ("s", ctypes.c_void_p), ("c", ctypes.c_void_p)]
+
+
+# name -> argtypes (all return gnss_status unless listed in _RESTYPES)
+_VP = ctypes.c_void_p
+_SIGS = {
+    "gnss_create": [ctypes.POINTER(GnssConfig), ctypes.POINTER(ctypes.c_void_p)],
+    "gnss_destroy": [_VP],
+    "gnss_field_bytes": [_VP],
+    "gnss_workspace_bytes": [_VP],
+    "gnss_status_string": [ctypes.c_int],
+    "gnss_last_error": [_VP],
+    "gnss_forward": [_VP, _VP, _VP],
+    "gnss_inverse": [_VP, _VP, _VP],
+    "gnss_dealias": [_VP, _VP, _VP],
+    "gnss_vorticity": [_VP] + [_VP] * 6 + [_VP],
+    "gnss_gradient": [_VP] + [_VP] * 4 + [_VP],
+    "gnss_divergence": [_VP] + [_VP] * 4 + [_VP],
+    "gnss_make_rhs": [_VP] + [_VP] * 5 + [_VP],
+    "gnss_timestep": [_VP, ctypes.c_int, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields),
+                      ctypes.POINTER(GnssFields), _VP],
+    "gnss_update": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields), _VP],
+    "gnss_cross_product": [_VP] + [_VP] * 6 + [_VP],
+    "gnss_dot_product": [_VP] + [_VP] * 7 + [_VP],
+    "gnss_colloid_advection": [_VP] + [_VP] * 11 + [_VP],
+    "gnss_step": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields), ctypes.c_int, _VP],
+    "gnss_stats": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(ctypes.c_double), _VP],
+    "gnss_run_host": [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _VP],
+}
+_RESTYPES = {
+    "gnss_field_bytes": ctypes.c_size_t,
+    "gnss_workspace_bytes": ctypes.c_size_t,
+    "gnss_status_string": ctypes.c_char_p,
+    "gnss_last_error": ctypes.c_char_p,
+}
+
+_lib = None
+
+
+def load_library(path: Path | str | None = None) -> ctypes.CDLL:
+    """Load libgnss_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build the CUDA library first (python gnss-1_b200/build.py)")
+    lib = ctypes.CDLL(str(p))
+    for name, args in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _ptr(x) -> int | None:
+    """Device pointer of a torch tensor (or an int / None passthrough)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    dp = getattr(x, "data_ptr", None)
+    if dp is None:
+        raise TypeError(f"expected a torch CUDA tensor or a device pointer, got {type(x)!r}")
+    if not x.is_cuda:
+        raise TypeError("tensor must live on a CUDA device")
+    if not x.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return dp()
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except ImportError:
+            pass
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _fields(fs: Sequence | None) -> GnssFields | None:
+    if fs is None:
+        return None
+    p = [_ptr(f) for f in fs] + [None] * (5 - len(fs))
+    return GnssFields(*p[:5])
+
+
+class Context:
+    """One grid configuration on one device (replaces plan1dFFT/plan2dFFT and
+    the global state of the reference, fftfuncs.cu:133-231, declare.h)."""
+
+    def __init__(self, n: int | None = None, *, nx: int | None = None, ny: int | None = None,
+                 nz: int | None = None, lx: float = 2 * math.pi, ly: float = 2 * math.pi,
+                 lz: float = 2 * math.pi, re: float = 1000.0, sc: float = 0.7, sc_c: float = 0.7,
+                 alpha: float = 0.0, dt: float = 1e-3, alias_filter: float = 2.0 / 3.0,
+                 nu_stats: float | None = None, n_scalars: int = 1, scheme: int = GNSS_SCHEME_CNAB2,
+                 precision: int = GNSS_FP64, device: int = 0):
+        self.lib = load_library()
+        nx, ny, nz = nx or n, ny or n, nz or n
+        if nu_stats is None:
+            nu_stats = 1.0 / re   # the reference's nu = H/Re with H = 1 (dnsparams.h:30)
+        self.cfg = GnssConfig(nx, ny, nz, lx, ly, lz, re, sc, sc_c, alpha, dt, alias_filter, nu_stats,
+                              n_scalars, scheme, precision, device)
+        h = ctypes.c_void_p()
+        st = self.lib.gnss_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_create", self.lib.gnss_status_string(st).decode())
+        self._h = h
+
+    # -- bookkeeping -------------------------------------------------------
+    @property
+    def nz2(self) -> int:
+        return self.cfg.nz // 2 + 1
+
+    @property
+    def spectral_shape(self) -> tuple:
+        return (self.cfg.ny, self.cfg.nx, self.nz2)
+
+    @property
+    def complex_dtype(self):
+        import torch
+        return torch.complex128 if self.cfg.precision == GNSS_FP64 else torch.complex64
+
+    @property
+    def n_fields(self) -> int:
+        return 3 + self.cfg.n_scalars
+
+    def field_bytes(self) -> int:
+        return int(self.lib.gnss_field_bytes(self._h))
+
+    def workspace_bytes(self) -> int:
+        return int(self.lib.gnss_workspace_bytes(self._h))
+
+    def empty_field(self, device=None):
+        import torch
+        return torch.zeros(self.spectral_shape, dtype=self.complex_dtype,
+                           device=device if device is not None else f"cuda:{self.cfg.device}")
+
+    def physical_view(self, t):
+        """Real padded view [nx, ny, 2*nz2] of a field tensor."""
+        import torch
+        return torch.view_as_real(t).reshape(self.cfg.nx, self.cfg.ny, 2 * self.nz2)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.gnss_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, st: int, what: str) -> None:
+        if st != GNSS_OK:
+            detail = self.lib.gnss_last_error(self._h)
+            raise GnssError(st, what, detail.decode() if detail else "")
+
+    # -- transforms (fftfuncs.cu:288-359) -----------------------------------
+    def forward_transform(self, f, stream=None) -> None:
+        self._ck(self.lib.gnss_forward(self._h, _ptr(f), _stream(stream)), "gnss_forward")
+
+    def inverse_transform(self, f, stream=None) -> None:
+        self._ck(self.lib.gnss_inverse(self._h, _ptr(f), _stream(stream)), "gnss_inverse")
+
+    # -- spectral / physical operators (solver.cu) --------------------------
+    def de_alias(self, fields: Iterable, stream=None) -> None:
+        for f in fields:
+            self._ck(self.lib.gnss_dealias(self._h, _ptr(f), _stream(stream)), "gnss_dealias")
+
+    def vorticity(self, u, v, w, o1, o2, o3, stream=None) -> None:
+        self._ck(self.lib.gnss_vorticity(self._h, *map(_ptr, (u, v, w, o1, o2, o3)), _stream(stream)),
+                 "gnss_vorticity")
+
+    def gradient(self, f, fx, fy, fz, stream=None) -> None:
+        self._ck(self.lib.gnss_gradient(self._h, *map(_ptr, (f, fx, fy, fz)), _stream(stream)), "gnss_gradient")
+
+    def divergence(self, fx, fy, fz, out, stream=None) -> None:
+        self._ck(self.lib.gnss_divergence(self._h, *map(_ptr, (fx, fy, fz, out)), _stream(stream)),
+                 "gnss_divergence")
+
+    def make_rhs(self, ru, rv, rw, rs=None, rc=None, stream=None) -> None:
+        self._ck(self.lib.gnss_make_rhs(self._h, *map(_ptr, (ru, rv, rw, rs, rc)), _stream(stream)),
+                 "gnss_make_rhs")
+
+    def timestep(self, euler: bool, state, rhs, rhs_old=None, stream=None) -> None:
+        so = _fields(rhs_old)
+        self._ck(self.lib.gnss_timestep(self._h, int(bool(euler)), ctypes.byref(_fields(state)),
+                                        ctypes.byref(_fields(rhs)), ctypes.byref(so) if so else None,
+                                        _stream(stream)), "gnss_timestep")
+
+    def update(self, rhs, rhs_old, stream=None) -> None:
+        self._ck(self.lib.gnss_update(self._h, ctypes.byref(_fields(rhs)), ctypes.byref(_fields(rhs_old)),
+                                      _stream(stream)), "gnss_update")
+
+    def cross_product(self, u, v, w, o1, o2, o3, stream=None) -> None:
+        self._ck(self.lib.gnss_cross_product(self._h, *map(_ptr, (u, v, w, o1, o2, o3)), _stream(stream)),
+                 "gnss_cross_product")
+
+    def dot_product(self, a, b, out, stream=None) -> None:
+        self._ck(self.lib.gnss_dot_product(self._h, *map(_ptr, (*a, *b, out)), _stream(stream)),
+                 "gnss_dot_product")
+
+    def colloid_advection(self, vel, c, grad_c, grad_s, lap_s_inout, stream=None) -> None:
+        args = (*vel, c, *grad_c, *grad_s, lap_s_inout)
+        self._ck(self.lib.gnss_colloid_advection(self._h, *map(_ptr, args), _stream(stream)),
+                 "gnss_colloid_advection")
+
+    # -- the step (solver.cu:700-765) ---------------------------------------
+    def solver_ps(self, state: Sequence, hist: Sequence | None, euler: bool, stream=None) -> None:
+        h = _fields(hist)
+        self._ck(self.lib.gnss_step(self._h, ctypes.byref(_fields(state)), ctypes.byref(h) if h else None,
+                                    int(bool(euler)), _stream(stream)), "gnss_step")
+
+    step = solver_ps
+
+    def stats(self, state: Sequence, stream=None) -> dict:
+        out = (ctypes.c_double * GNSS_NSTATS)()
+        self._ck(self.lib.gnss_stats(self._h, ctypes.byref(_fields(state)), out, _stream(stream)), "gnss_stats")
+        return dict(zip(STAT_NAMES, list(out)))
+
+    def run_host(self, host_in, host_out, n_steps: int, first_euler: bool = True, stats=None,
+                 stream=None) -> None:
+        """End-to-end call: host (ideally pinned) packed state in and out."""
+        sp = None
+        if stats is not None:
+            sp = stats.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if isinstance(stats, np.ndarray) \
+                else ctypes.cast(stats.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        self._ck(self.lib.gnss_run_host(self._h, _host_ptr(host_in), _host_ptr(host_out), int(n_steps),
+                                        int(bool(first_euler)), sp, _stream(stream)), "gnss_run_host")
+
+    # reference spellings
+    forwardTransform = forward_transform
+    inverseTransform = inverse_transform
+    deAlias = de_alias
+    makeRHS = make_rhs
+    crossProduct = cross_product
+    dotProduct = dot_product
+    colloidAdvection = colloid_advection
+
+
+def _host_ptr(x) -> int:
+    if isinstance(x, np.ndarray):
+        assert x.flags.c_contiguous
+        return x.ctypes.data
+    if isinstance(x, int):
+        return x
+    if x.is_cuda:
+        raise TypeError("run_host expects host memory")
+    return x.data_ptr()
+
+
+# ---------------------------------------------------------------- initial state
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    x = (x + np.uint64(0x9E3779B97F4A7C15)).astype(np.uint64)
+    z = x
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def _normals(seed: int, keys: np.ndarray) -> np.ndarray:
+    """Counter-based standard normals: one per uint64 key, reproducible on any machine."""
+    with np.errstate(over="ignore"):
+        s = _splitmix64(np.array([seed], dtype=np.uint64))[0]
+        k2 = keys.astype(np.uint64) * np.uint64(2)
+        a = _splitmix64(k2 ^ s)
+        b = _splitmix64((k2 + np.uint64(1)) ^ s)
+    u1 = ((a >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    u2 = ((b >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+
+
+def jet_profile(ny: int, ly: float, h: float = 1.0, theta: float = 0.05) -> np.ndarray:
+    """Temporal-jet profile on the y grid (initialize.cu:114-136, 161-177):
+    0.5 - 0.5 tanh(H/(4 theta) (2|y|/H - 1)) with y = -ly/2 + j ly/ny."""
+    y = -ly / 2 + np.arange(ny) * ly / ny
+    return 0.5 - 0.5 * np.tanh(h / (4.0 * theta) * (2.0 * np.abs(y) / h - 1.0))
+
+
+def jet_initial_state(nx: int, ny: int | None = None, nz: int | None = None, *, lx: float = 2 * math.pi,
+                      ly: float = 2 * math.pi, lz: float = 2 * math.pi, n_scalars: int = 1, seed: int = 0,
+                      noise_kmax: float = 8.0, amp: float = 0.05, h: float = 1.0, theta: float = 0.05,
+                      dtype=np.complex128) -> list:
+    """Seeded spectral initial state [u, v, w, s(, c)], each complex [ny][nx][nz2].
+
+    u = U(y) + noise, v, w = noise, s (and c) = U(y).  The noise is the
+    solenoidal field i k x A on the modes 0 < |k| <= noise_kmax with A drawn
+    from a counter-based generator keyed by ``seed``, Hermitian in the kz = 0
+    plane, scaled so that the mean component rms in physical space is ``amp``.
+    """
+    ny = ny or nx
+    nz = nz or nx
+    nz2 = nz // 2 + 1
+    nn = float(nx) * ny * nz
+    dkx, dky, dkz = 2 * math.pi / lx, 2 * math.pi / ly, 2 * math.pi / lz
+    fields = [np.zeros((ny, nx, nz2), dtype=dtype) for _ in range(3 + n_scalars)]
+    prof = np.fft.fft(jet_profile(ny, ly, h, theta)) * (nx * nz)
+    fields[0][:, 0, 0] = prof
+    for q in range(3, 3 + n_scalars):
+        fields[q][:, 0, 0] = prof
+    if amp > 0 and noise_kmax > 0:
+        kx_n = int(math.floor(noise_kmax / dkx))
+        ky_n = int(math.floor(noise_kmax / dky))
+        kz_n = int(math.floor(noise_kmax / dkz))
+        kx_n = min(kx_n, nx // 2 - 1)
+        ky_n = min(ky_n, ny // 2 - 1)
+        kz_n = min(kz_n, nz // 2 - 1)
+        mx, my, mz = np.meshgrid(np.arange(-kx_n, kx_n + 1), np.arange(-ky_n, ky_n + 1), np.arange(0, kz_n + 1),
+                                 indexing="ij")
+        mx, my, mz = mx.ravel(), my.ravel(), mz.ravel()
+        kx, ky, kz = mx * dkx, my * dky, mz * dkz
+        k2 = kx * kx + ky * ky + kz * kz
+        canon = (mz > 0) | ((mz == 0) & ((my > 0) | ((my == 0) & (mx > 0))))
+        sel = (k2 > 0) & (k2 <= noise_kmax ** 2 * (1 + 1e-12)) & canon
+        mx, my, mz, kx, ky, kz = mx[sel], my[sel], mz[sel], kx[sel], ky[sel], kz[sel]
+        base = ((mx + 1024).astype(np.int64) * 2048 + (my + 1024)) * 2048 + mz
+        a = np.empty((3, mx.size), dtype=np.complex128)
+        for comp in range(3):
+            re_ = _normals(seed, base * 8 + 2 * comp)
+            im_ = _normals(seed, base * 8 + 2 * comp + 1)
+            a[comp] = (re_ + 1j * im_) / math.sqrt(2.0)
+        kv = np.stack([kx, ky, kz])
+        # n = i k x A
+        cross = np.stack([ky * a[2] - kz * a[1], kz * a[0] - kx * a[2], kx * a[1] - ky * a[0]])
+        nh = 1j * cross
+        wt = np.where(mz > 0, 2.0, 1.0)
+        # mirrored kz = 0 modes contribute once more
+        wt = np.where(mz == 0, 2.0, wt)
+        var = (wt * np.abs(nh) ** 2).sum(axis=1) / nn ** 2
+        scale = amp / math.sqrt(var.mean()) if var.mean() > 0 else 0.0
+        nh *= scale
+        iy, ix = my % ny, mx % nx
+        for comp in range(3):
+            fields[comp][iy, ix, mz] += nh[comp].astype(dtype)
+            z0 = mz == 0
+            fields[comp][(-my[z0]) % ny, (-mx[z0]) % nx, 0] += np.conj(nh[comp][z0]).astype(dtype)
+        del kv
+    return fields
+
+
+def pack_state(fields: Sequence[np.ndarray], out: np.ndarray | None = None) -> np.ndarray:
+    """Back-to-back copy of fields (the layout gnss_run_host expects)."""
+    n = fields[0].size
+    if out is None:
+        out = np.empty(n * len(fields), dtype=fields[0].dtype)
+    for q, f in enumerate(fields):
+        out[q * n:(q + 1) * n] = f.ravel()
+    return out

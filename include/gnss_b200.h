@@ -1,0 +1,157 @@
+/*
+ * gnss_b200.h -- C ABI of the B200-native pseudospectral temporal-jet step.
+ *
+ * Drop-in for the operator surface of the reference solver (mfkiwl/gnss-1):
+ * the 3D transforms of fftfuncs.cu and the spectral / physical operators and
+ * time step of solver.cu.  Every entry point cites the reference function it
+ * replaces.  Buffers use the reference's layouts:
+ *
+ *   spectral field  complex [ny][nx][nz2], index kz + nz2*(x + nx*y)   (solver.cu:25)
+ *   physical field  real    [nx][ny][2*nz2], index z + 2*nz2*(y + ny*x) (cudafuncs.cu:14-17)
+ *
+ * with nz2 = nz/2 + 1; a field buffer holds nx*ny*nz2 complex values and is
+ * used in place for both views, exactly like the reference.  Element type is
+ * double (GNSS_FP64) or float (GNSS_FP32) per the context's precision.
+ *
+ * Differences from the reference, all deliberate:
+ *   - sizes and parameters are runtime values (gnss_config) instead of the
+ *     compile-time macros of dnsparams.h;
+ *   - every call takes an explicit CUDA stream (cudaStream_t passed as void*,
+ *     NULL = legacy default stream) and returns a gnss_status instead of
+ *     printing and returning void;
+ *   - scratch memory (the reference's fft.temp / fft.wspace / rhs / temp
+ *     buffers) is owned by the context.
+ *
+ * Thread safety: a context may be used by one host thread at a time; calls
+ * on one context are ordered on the stream they are given.
+ */
+#ifndef GNSS_B200_H
+#define GNSS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gnss_status;
+#define GNSS_OK 0
+#define GNSS_ERR_INVALID 1       /* bad argument, unsupported size or configuration */
+#define GNSS_ERR_CUDA 2          /* a CUDA runtime call or kernel launch failed       */
+#define GNSS_ERR_NOMEM 3         /* device or pinned allocation failed                */
+#define GNSS_ERR_UNSUPPORTED 4   /* operation not available for this configuration    */
+
+#define GNSS_SCHEME_CNAB2 0      /* reference scheme: Euler/CN first step, AB2/CN after (solver.cu:547-616) */
+#define GNSS_SCHEME_RK3IF 1      /* low-storage RK3 (Wray) with integrating factor exp(-nu k^2 dt)          */
+
+#define GNSS_FP64 0
+#define GNSS_FP32 1
+
+typedef struct gnss_config {
+    int nx, ny, nz;          /* grid; each 2^a 3^b, even, 8..512                                */
+    double lx, ly, lz;       /* box lengths (reference LX, LY, LZ)                              */
+    double re;               /* velocity diffusivity 1/re (reference Re)                        */
+    double sc;               /* scalar s diffusivity 1/(re*sc) (reference Sc)                   */
+    double sc_c;             /* scalar c diffusivity 1/(re*sc_c) (reference Sc_c)               */
+    double alpha;            /* drift coefficient of c (reference alpha)                        */
+    double dt;               /* time step (reference dt)                                        */
+    double alias_filter;     /* modes with k^2 > (alias_filter*nx*pi/lx)^2 are zeroed           */
+    double nu_stats;         /* viscosity used by the statistics (reference nu = H/Re)          */
+    int n_scalars;           /* 1: s only; 2: s and c                                          */
+    int scheme;              /* GNSS_SCHEME_*                                                   */
+    int precision;           /* GNSS_FP64 or GNSS_FP32                                          */
+    int device;              /* CUDA device ordinal                                             */
+} gnss_config;
+
+/* Device pointers to the spectral fields of one state (or one set of RHS /
+ * history fields).  c may be NULL when n_scalars == 1. */
+typedef struct gnss_fields {
+    void *u, *v, *w, *s, *c;
+} gnss_fields;
+
+typedef struct gnss_ctx gnss_ctx;
+
+/* Statistics written by gnss_stats (statistics.cu:1494-1845 definitions). */
+#define GNSS_STAT_KE 0       /* 1/2 sum |u_hat|^2 / NN^2             (calcVrms, statistics.cu:1549)            */
+#define GNSS_STAT_VRMS2 1    /* sum |u_hat|^2 / (3 NN^2)             (calcVrms, statistics.cu:1551)            */
+#define GNSS_STAT_EPS 2      /* nu_stats sum k^2 |u_hat|^2 / NN^2    (calcEpsilonKernel, statistics.cu:1637)   */
+#define GNSS_STAT_CHI_S 3    /* 2 nu_stats/sc sum k^2|s_hat|^2/NN^2  (calcScalarDissipation, statistics.cu:1813) */
+#define GNSS_STAT_CHI_C 4    /* same for c with sc_c                                                              */
+#define GNSS_STAT_VAR_S 5    /* sum_{k != 0} |s_hat|^2 / NN^2        (scalar variance; not in the reference)     */
+#define GNSS_STAT_VAR_C 6
+#define GNSS_NSTATS 7
+
+/* Create a context: validates the configuration, builds twiddle tables and
+ * wavenumber constants.  Replaces plan1dFFT / plan2dFFT (fftfuncs.cu:133-231)
+ * and initializeWaveNumbers (initialize.cu:693-707). */
+gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out);
+/* Release a context and all memory it owns (cufftDestroy in allocate.cu:297-301). */
+gnss_status gnss_destroy(gnss_ctx *ctx);
+/* Bytes of one field buffer (nx*ny*nz2 complex of the context's precision). */
+size_t gnss_field_bytes(const gnss_ctx *ctx);
+/* Bytes of device memory the context owns right now. */
+size_t gnss_workspace_bytes(const gnss_ctx *ctx);
+const char *gnss_status_string(gnss_status st);
+/* Human-readable description of the last error seen by this context. */
+const char *gnss_last_error(const gnss_ctx *ctx);
+
+/* 3D transforms, in place on one field buffer.
+ * forward: physical -> spectral, unnormalised   (forwardTransform, fftfuncs.cu:288-320)
+ * inverse: spectral -> physical, scaled by 1/(nx ny nz) (inverseTransform, fftfuncs.cu:322-359) */
+gnss_status gnss_forward(gnss_ctx *ctx, void *field, void *stream);
+gnss_status gnss_inverse(gnss_ctx *ctx, void *field, void *stream);
+
+/* Spectral operators on spectral fields. */
+gnss_status gnss_dealias(gnss_ctx *ctx, void *field, void *stream);                 /* deAliasKernel_mgpu, solver.cu:17-42  */
+gnss_status gnss_vorticity(gnss_ctx *ctx, const void *uh, const void *vh, const void *wh,
+                           void *o1, void *o2, void *o3, void *stream);             /* vorticity, solver.cu:68-137           */
+gnss_status gnss_gradient(gnss_ctx *ctx, const void *fh, void *fx, void *fy, void *fz,
+                          void *stream);                                              /* gradient, solver.cu:233-273           */
+gnss_status gnss_divergence(gnss_ctx *ctx, const void *fx, const void *fy, const void *fz,
+                            void *out, void *stream);                                 /* divergence, solver.cu:275-307         */
+gnss_status gnss_make_rhs(gnss_ctx *ctx, void *ru, void *rv, void *rw, void *rs, void *rc,
+                          void *stream);                                              /* makeRHS, solver.cu:461-544            */
+/* CN time update of every field of `state` from `rhs` (and `rhs_old` when
+ * euler == 0) (timestep, solver.cu:547-616). */
+gnss_status gnss_timestep(gnss_ctx *ctx, int euler, const gnss_fields *state, const gnss_fields *rhs,
+                          const gnss_fields *rhs_old, void *stream);
+/* rhs_old <- rhs; rhs <- 0 (update, solver.cu:618-657). */
+gnss_status gnss_update(gnss_ctx *ctx, const gnss_fields *rhs, const gnss_fields *rhs_old, void *stream);
+
+/* Physical-space operators on physical (real, padded) fields. */
+gnss_status gnss_cross_product(gnss_ctx *ctx, const void *u, const void *v, const void *w,
+                               void *o1, void *o2, void *o3, void *stream);       /* crossProduct: o <- o x u, solver.cu:139-185 */
+gnss_status gnss_dot_product(gnss_ctx *ctx, const void *a1, const void *a2, const void *a3,
+                             const void *b1, const void *b2, const void *b3, void *out,
+                             void *stream);                                          /* dotProduct, solver.cu:342-372 */
+gnss_status gnss_colloid_advection(gnss_ctx *ctx, const void *u, const void *v, const void *w,
+                                   const void *c, const void *cx, const void *cy, const void *cz,
+                                   const void *sx, const void *sy, const void *sz, void *lap_s_inout,
+                                   void *stream);                                    /* colloidAdvection, solver.cu:374-405 */
+
+/* One full time step of the fused B200 path (solver_ps, solver.cu:700-765).
+ * state: spectral u, v, w, s (and c).  hist: for GNSS_SCHEME_CNAB2 the
+ * previous RHS (the reference's rhs_old; read when euler == 0, always
+ * written); unused (may be NULL) for GNSS_SCHEME_RK3IF.  euler selects the
+ * reference's first-step Euler/CN update (main.cu:181-186). */
+gnss_status gnss_step(gnss_ctx *ctx, const gnss_fields *state, const gnss_fields *hist, int euler, void *stream);
+
+/* Spectral statistics of a state; writes GNSS_NSTATS doubles to host memory
+ * and synchronises the stream (calcVrms, calcDissipationRate,
+ * calcScalarDissipationRate: statistics.cu:1494-1845). */
+gnss_status gnss_stats(gnss_ctx *ctx, const gnss_fields *state, double *out, void *stream);
+
+/* End-to-end call with host buffers: copies the packed host state
+ * (3 + n_scalars spectral fields back to back) to context-owned device
+ * buffers, runs n_steps steps (the first one Euler when first_euler != 0 for
+ * GNSS_SCHEME_CNAB2; hist starts at zero), records the statistics after each
+ * step into stats_out (n_steps * GNSS_NSTATS doubles, may be NULL) and copies
+ * the final state back into host_state_out (may alias host_state_in).
+ * Synchronises the stream before returning. */
+gnss_status gnss_run_host(gnss_ctx *ctx, const void *host_state_in, void *host_state_out, int n_steps,
+                          int first_euler, double *stats_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GNSS_B200_H */

@@ -1,0 +1,156 @@
+"""The fused CUDA time step (gnss_step) against the oracle's restatement of
+solver_ps (solver.cu:700-765) and of the IF-RK3 scheme, plus statistics.
+
+Tolerances: FP64 relative L2 per field <= 1e-12 after one step and <= 1e-11
+after several (round-off growth only); statistics within 1e-10 relative;
+FP32 step within 1e-5 relative L2 of the FP64 oracle after 10 steps.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from _util import rel_l2, to_dev, to_host
+
+CASES = [
+    # name, n, re, sc, sc_c, alpha, dt, n_scalars
+    ("k16_1s", 16, 200.0, 0.7, 1.0, 0.0, 2e-3, 1),
+    ("k16_2s", 16, 200.0, 0.7, 1.0, 0.0, 2e-3, 2),
+    ("k16_alpha", 16, 200.0, 0.7, 1.0, 0.05, 2e-3, 2),
+    ("k24_2s", 24, 300.0, 1.0, 2.0, 0.0, 1e-3, 2),
+    ("c64", 64, 1000.0, 0.7, 0.7, 0.0, 1e-3, 1),
+]
+
+
+def _initial(G, n, n_scalars, seed=0, kmax=None):
+    kmax = kmax if kmax is not None else min(8.0, n / 4)
+    return G.jet_initial_state(n, n_scalars=n_scalars, seed=seed, noise_kmax=kmax, amp=0.05)
+
+
+def _oracle_run(oracle, oc, init, n_scalars, nsteps):
+    f = [a.copy() for a in init] + ([np.zeros_like(init[0])] if n_scalars == 1 else [])
+    r = [np.zeros_like(init[0]) for _ in range(5)]
+    out = []
+    for s in range(nsteps):
+        oracle.step_cnab2(oc, f, r, euler=(s == 0))
+        out.append(([a.copy() for a in f], oracle.stats(oc, f)))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_step_cnab2_fp64(torch_cuda, oracle, case):
+    import gnss_b200 as G
+    torch = torch_cuda
+    name, n, re, sc, scc, al, dt, ns = case
+    nsteps = 3 if n >= 64 else 5
+    init = _initial(G, n, ns)
+    oc = oracle.cfg(n, re=re, sc=sc, sc_c=scc, alpha=al, dt=dt)
+    ref = _oracle_run(oracle, oc, init, ns, nsteps)
+    with G.Context(n, re=re, sc=sc, sc_c=scc, alpha=al, dt=dt, n_scalars=ns) as ctx:
+        st = [to_dev(torch, a) for a in init]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        # the reference dealiases the state once before the loop (main.cu:156)
+        ctx.de_alias(st)
+        for s in range(nsteps):
+            ctx.solver_ps(st, hi, euler=(s == 0))
+            stats = ctx.stats(st)
+            fields, rstats = ref[s]
+            tol = 1e-12 if s == 0 else 1e-11
+            for q in range(3 + ns):
+                err = rel_l2(to_host(st[q]), fields[q])
+                assert err < tol, f"step {s + 1} field {q}: rel L2 {err:.3e}"
+            for k in ("ke", "eps", "chi_s", "var_s") + (("chi_c", "var_c") if ns == 2 else ()):
+                assert math.isclose(stats[k], rstats[k], rel_tol=1e-10), (s, k, stats[k], rstats[k])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ns", [1, 2])
+def test_step_rk3if_fp64(torch_cuda, oracle, ns):
+    import gnss_b200 as G
+    torch = torch_cuda
+    n, re, dt = 24, 400.0, 2e-3
+    init = _initial(G, n, ns, seed=3)
+    oc = oracle.cfg(n, re=re, sc=0.7, sc_c=1.3, dt=dt)
+    f = [a.copy() for a in init]
+    with G.Context(n, re=re, sc=0.7, sc_c=1.3, dt=dt, n_scalars=ns, scheme=G.GNSS_SCHEME_RK3IF) as ctx:
+        st = [to_dev(torch, a) for a in init]
+        for s in range(4):
+            oracle.step_rk3if(oc, f, ns)
+            ctx.solver_ps(st, None, euler=False)
+            for q in range(3 + ns):
+                err = rel_l2(to_host(st[q]), f[q])
+                assert err < 1e-12, f"step {s + 1} field {q}: rel L2 {err:.3e}"
+
+
+@pytest.mark.gpu
+def test_step_fp32_error_budget(torch_cuda, oracle):
+    """FP32 storage and transforms stay within 1e-5 relative L2 of FP64 after 10 steps."""
+    import gnss_b200 as G
+    torch = torch_cuda
+    n, re, dt, ns = 32, 1000.0, 1e-3, 1
+    init = _initial(G, n, ns)
+    with G.Context(n, re=re, dt=dt, n_scalars=ns) as c64, \
+            G.Context(n, re=re, dt=dt, n_scalars=ns, precision=G.GNSS_FP32) as c32:
+        a = [to_dev(torch, x) for x in init]
+        ha = [torch.zeros_like(a[0]) for _ in a]
+        b = [to_dev(torch, x.astype(np.complex64)) for x in init]
+        hb = [torch.zeros_like(b[0]) for _ in b]
+        c64.de_alias(a)
+        c32.de_alias(b)
+        for s in range(10):
+            c64.solver_ps(a, ha, euler=(s == 0))
+            c32.solver_ps(b, hb, euler=(s == 0))
+        torch.cuda.synchronize()
+        for q in range(3 + ns):
+            err = rel_l2(to_host(b[q]).astype(np.complex128), to_host(a[q]))
+            assert err < 1e-5, f"field {q}: {err:.3e}"
+
+
+@pytest.mark.gpu
+def test_taylor_green_decay(torch_cuda):
+    """2D Taylor-Green vortex: an exact solution; CN gives a known amplitude factor per step."""
+    import gnss_b200 as G
+    torch = torch_cuda
+    n, re, dt, steps = 32, 100.0, 1e-2, 20
+    x = np.arange(n) * 2 * np.pi / n
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    with G.Context(n, re=re, dt=dt, n_scalars=1) as ctx:
+        phys = [np.sin(X) * np.cos(Y), -np.cos(X) * np.sin(Y), 0 * X, np.cos(2 * Z)]
+        from _util import phys_to_buffer
+        st = [to_dev(torch, phys_to_buffer(p)) for p in phys]
+        for t in st:
+            ctx.forward_transform(t)
+        a0 = to_host(st[0]).copy()
+        s0 = to_host(st[3]).copy()
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        for s in range(steps):
+            ctx.solver_ps(st, hi, euler=(s == 0))
+        torch.cuda.synchronize()
+        a = dt / re                       # dt/2 * k^2 / Re with k^2 = 2
+        assert rel_l2(to_host(st[0]), a0 * ((1 - a) / (1 + a)) ** steps) < 1e-13
+        b = dt / 2 * 4 / (re * 0.7)
+        assert rel_l2(to_host(st[3]), s0 * ((1 - b) / (1 + b)) ** steps) < 1e-13
+
+
+@pytest.mark.gpu
+def test_run_host_matches_device_steps(torch_cuda):
+    """The end-to-end host-buffer call equals the same steps on device buffers."""
+    import gnss_b200 as G
+    torch = torch_cuda
+    n, ns, steps = 32, 2, 4
+    init = _initial(G, n, ns, seed=7)
+    with G.Context(n, n_scalars=ns, re=800.0, dt=1e-3) as ctx:
+        st = [to_dev(torch, a) for a in init]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        for s in range(steps):
+            ctx.solver_ps(st, hi, euler=(s == 0))
+        last = ctx.stats(st)
+        host = torch.from_numpy(G.pack_state(init)).pin_memory()
+        out = torch.empty_like(host).pin_memory()
+        stats = np.zeros((steps, G.GNSS_NSTATS))
+        ctx.run_host(host, out, steps, True, stats)
+        got = out.numpy().reshape(len(init), *init[0].shape)
+        for q in range(len(init)):
+            assert rel_l2(got[q], to_host(st[q])) < 1e-14
+        assert math.isclose(stats[-1][0], last["ke"], rel_tol=1e-13)
