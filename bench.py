@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Throughput of the pseudospectral temporal-jet step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 512] [--precision mixed|fp64] [--scheme cnab2|rk3if]
+
+Workload (default): one 512^3 periodic temporal jet, U(y) = 0.5(1+tanh((0.5-|y-pi|)/0.1)),
+one scalar with the same profile, seeded solenoidal noise of rms 0.05 on |k| <= 8,
+Re 5000, Sc 0.7, dt 2.5e-4, 2/3 dealiasing, the reference's Euler/AB2 + Crank-Nicolson
+scheme; state resident on the device.  A step is one full time step (nonlinear term,
+projection, dealiasing, update).  Metric: Mpoint-steps/s = N^3 * steps / s / 1e6,
+summed over GPUs (each GPU advances its own jet: replicas, no collective).
+
+Rank 0 prints one JSON line.  Inputs (>= 1 GB per field) exceed L2 (126 MB), so no
+flush is needed between steps.  --impl reference runs the reference's own CUDA step
+(oracle/_ref/c512/refdrv built from the unmodified sources) on the same grid.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "gnss-1_b200"))
+
+METRIC = "Mpoint-steps/s at 512^3 (mixed precision; FP64 alongside)"
+UNIT = "Mpoint-steps/s"
+RE, SC, DT, NOISE_K, AMP = 5000.0, 0.7, 2.5e-4, 8.0, 0.05
+E2E_STEPS_PER_CALL = 20
+
+
+# ------------------------------------------------------------------ utilities
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if gpu_index < len(ids):
+                gpu_index = ids[gpu_index]
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.out.flush()
+        rows = []
+        try:
+            with open(self.out.name) as fp:
+                for line in fp:
+                    p = [x.strip() for x in line.split(",")]
+                    if len(p) >= 9:
+                        rows.append(p)
+        finally:
+            os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# stage -> (fields read, fields written) of one launch in the fused step, per the pass structure
+def stage_traffic(nphys: int, nnl: int, nf: int) -> dict:
+    return {
+        "x_inverse": (nf, nphys),          # state (dealiased, derivatives formed on load) -> quantities
+        "y_inverse": (nphys, nphys),
+        "z_physical": (nphys, nnl),        # physical products never leave the chip
+        "y_forward": (nnl, nnl),
+        "x_forward": (nnl, nnl),
+        "spectral_update": (nnl + 2 * nf, 2 * nf),   # nonlinear, state, history -> state, history
+    }
+
+
+def counts(n_scalars: int, alpha: float = 0.0):
+    nphys = 9 + (3 if n_scalars > 1 else 0) + (2 if (n_scalars > 1 and alpha != 0.0) else 0)
+    nnl = 3 + n_scalars
+    return nphys, nnl, 3 + n_scalars
+
+
+# ------------------------------------------------------------------ our arm
+def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None):
+    """Time `steps` steps of one jet resident on `dev`; returns a dict."""
+    cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
+    init = G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
+    ctx = G.Context(n, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme, device=dev)
+    st = [torch.from_numpy(a.astype(cdt)).to(f"cuda:{dev}") for a in init]
+    del init
+    hi = [torch.zeros_like(st[0]) for _ in st] if scheme == G.GNSS_SCHEME_CNAB2 else None
+    ctx.de_alias(st)
+    for s in range(warmup):
+        ctx.solver_ps(st, hi, euler=(s == 0))
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if barrier:
+        barrier()
+    torch.cuda.synchronize(dev)
+    l0 = ctx.launch_count()
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for s in range(steps):
+            ctx.solver_ps(st, hi, euler=(warmup == 0 and s == 0))
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    if barrier:
+        barrier()
+    launches = ctx.launch_count() - l0
+    ms = e0.elapsed_time(e1) / steps
+    stats = ctx.stats(st)
+    # per-stage device times (separate profiled steps of the same workload)
+    ctx.profile(True)
+    for s in range(profile_steps):
+        ctx.solver_ps(st, hi, euler=False)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    out = dict(ms=ms, launches=launches, clocks=clk.summary(), stats=stats, profile=prof,
+               field_bytes=ctx.field_bytes())
+    del st, hi
+    ctx.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_e2e(G, torch, n, precision, scheme, calls, dev):
+    """Public host-buffer API: pinned state in, E2E_STEPS_PER_CALL steps, state and statistics out."""
+    cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
+    init = [a.astype(cdt) for a in G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)]
+    ctx = G.Context(n, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme, device=dev)
+    host_in = torch.from_numpy(G.pack_state(init)).pin_memory()
+    del init
+    host_out = torch.empty_like(host_in).pin_memory()
+    stats = np.zeros((E2E_STEPS_PER_CALL, G.GNSS_NSTATS))
+    ctx.run_host(host_in, host_out, E2E_STEPS_PER_CALL, True, stats)   # warm-up call
+    stream = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(calls):
+        ctx.run_host(host_in, host_out, E2E_STEPS_PER_CALL, True, stats)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_call = e0.elapsed_time(e1) / calls
+    state_bytes = host_in.numel() * host_in.element_size()
+    ctx.close()
+    del host_in, host_out
+    return dict(ms_call=ms_call, h2d=state_bytes / E2E_STEPS_PER_CALL,
+                d2h=(state_bytes + E2E_STEPS_PER_CALL * G.GNSS_NSTATS * 8) / E2E_STEPS_PER_CALL)
+
+
+def cpu_baseline(n_sample=256, steps=2) -> dict:
+    """The CPU oracle (same scheme and parameters) on all host cores, bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    import gnss_b200 as G
+    O.build()
+    cores = os.cpu_count() or 1
+    oc = O.cfg(n_sample, re=RE, sc=SC, dt=DT, nthreads=cores)
+    f = G.jet_initial_state(n_sample, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
+    f.append(np.zeros_like(f[0]))
+    r = [np.zeros_like(f[0]) for _ in range(5)]
+    t0 = time.perf_counter()
+    for s in range(steps):
+        O.step_cnab2(oc, f, r, euler=(s == 0))
+    dt = time.perf_counter() - t0
+    return {"value": round(n_sample ** 3 * steps / dt / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} FP64 steps of the reference scheme (29 transforms/step, the reference's own "
+                      f"sequence, solver.cu:700-765) at {n_sample}^3 with the same parameters, "
+                      f"{dt:.1f} s on {cores} threads"}
+
+
+def ours(args):
+    import torch
+    import gnss_b200 as G
+    ws, rank, local = dist_env()
+    dev = local
+    torch.cuda.set_device(dev)
+    barrier = None
+    red = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{dev}"))
+        barrier = dist.barrier
+
+        def red(x, op="max"):
+            t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+            return float(t.item())
+    prec = G.GNSS_FP32 if args.precision == "mixed" else G.GNSS_FP64
+    scheme = G.GNSS_SCHEME_CNAB2 if args.scheme == "cnab2" else G.GNSS_SCHEME_RK3IF
+    n = args.n
+    leg = run_leg(G, torch, n, prec, scheme, args.steps, args.warmup, dev, barrier=barrier)
+    ms = leg["ms"] if red is None else red(leg["ms"])
+    pts = float(n) ** 3
+    value = ws * pts / (ms * 1e-3) / 1e6
+    fp64 = None
+    if prec == G.GNSS_FP32 and not args.no_fp64_leg:
+        l64 = run_leg(G, torch, n, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier)
+        ms64 = l64["ms"] if red is None else red(l64["ms"])
+        fp64 = {"value": round(ws * pts / (ms64 * 1e-3) / 1e6, 3), "ms_per_step": round(ms64, 4),
+                "mixed_over_fp64": round(ms64 / ms, 3)}
+    e2e = None
+    if not args.no_e2e:
+        e = run_e2e(G, torch, n, prec, scheme, args.e2e_calls, dev)
+        ms_call = e["ms_call"] if red is None else red(e["ms_call"])
+        e2e = {"value": round(ws * pts * E2E_STEPS_PER_CALL / (ms_call * 1e-3) / 1e6, 3), "unit": UNIT,
+               "h2d_bytes_per_step": int(e["h2d"]), "d2h_bytes_per_step": int(e["d2h"]),
+               "steps_per_call": E2E_STEPS_PER_CALL,
+               "call": "gnss_run_host: pinned host state in, steps, per-step statistics and state out"}
+    # roofline of the dominant kernel (stage of the fused step with the largest device time)
+    nphys, nnl, nf = counts(1)
+    traffic = stage_traffic(nphys, nnl, nf)
+    prof = leg["profile"]
+    dom = max(prof, key=lambda k: prof[k][0])
+    t_ms, nl = prof[dom]
+    rd, wr = traffic[dom]
+    alg = (rd + wr) * leg["field_bytes"]
+    peaks = measured_peaks()
+    achieved = alg / (t_ms / nl * 1e-3) / 1e9
+    tr_file = ROOT / "profiles" / "traffic.json"
+    traffic_meas = None
+    if tr_file.exists():
+        tj = json.loads(tr_file.read_text())
+        key = f"{args.precision}:{n}:{dom}"
+        if key in tj:
+            traffic_meas = tj[key]
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic_meas,
+                "algorithmic_bytes": int(alg), "peak_source": peaks["source"] + " (burst copy)",
+                "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()}}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec == G.GNSS_FP32 else "f64", "data": "synthetic",
+        "config": {"workload": f"temporal jet {n}^3, 1 scalar, Re {RE:g}, Sc {SC}, dt {DT:g}, "
+                               f"noise |k|<={NOISE_K:g} rms {AMP}, 2/3 dealias, {args.scheme}",
+                   "grid": n, "precision": args.precision, "scheme": args.scheme,
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (>= 0.5 GB per field); no flush"},
+        "gpu_launches": leg["launches"], "clocks": leg["clocks"], "e2e": e2e, "roofline": roofline,
+        "cpu_baseline": cpu, "fp64": fp64,
+        "stats_after": {k: leg["stats"][k] for k in ("ke", "eps", "chi_s", "var_s")},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ reference arm
+def reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    exe = ROOT / "oracle" / "_ref" / f"c{args.n}" / "refdrv"
+    if not exe.exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build {exe} missing "
+                                                             f"(oracle/build_ref.sh)"}))
+        return
+    r = subprocess.run([str(exe), "time", str(args.steps), str(args.warmup)], capture_output=True, text=True,
+                       timeout=3600, env=dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get(
+                           "CUDA_VISIBLE_DEVICES", str(local))))
+    if r.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": f"refdrv failed: {r.stderr.strip()[-200:]}"}))
+        return
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    ms = float(d["ms_per_step"])
+    value = float(args.n) ** 3 / (ms * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "impl": "reference", "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"temporal jet {args.n}^3, Re {RE:g}, Sc {SC}, dt {DT:g}, 2/3 dealias, cnab2 "
+                               f"(reference solver_ps; always carries both scalars s and c)",
+                   "grid": args.n, "precision": "fp64", "scheme": "cnab2", "parallelism": "single GPU"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "the reference's own CUDA step (cuFFT, sm_100a build of the unmodified "
+                                   "sources, one host thread driving the GPU); the reference has no CPU "
+                                   f"implementation of this path; {args.steps} timed steps after "
+                                   f"{args.warmup} warm-up"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--scheme", choices=("cnab2", "rk3if"), default="cnab2")
+    ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64-leg", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("bench.py: at least 3 warm-up steps are required", file=sys.stderr)
+        args.warmup = 3
+    if args.impl == "reference":
+        reference(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -31,6 +31,40 @@ struct gnss_ctx {
     int nphys = 0, nnl = 0;                       // quantities in the physical pass, nonlinear outputs
     RecipeSet recipes{};
     std::string err;
+    long long launches = 0;                       // kernels launched by this context
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;             // profiling events, reused
+    std::vector<std::pair<int, std::pair<int, int>>> ev_rec;   // (stage, (start event, end event))
+};
+
+// Records an event pair around one stage launch when profiling is on.
+struct StageTimer {
+    gnss_ctx *c;
+    cudaStream_t s;
+    int stage, e0 = -1;
+    StageTimer(gnss_ctx *c_, cudaStream_t s_, int st) : c(c_), s(s_), stage(st) {
+        c->launches++;
+        if (c->profiling) {
+            e0 = take();
+            cudaEventRecord(c->ev_pool[e0], s);
+        }
+    }
+    ~StageTimer() {
+        if (e0 >= 0) {
+            int e1 = take();
+            cudaEventRecord(c->ev_pool[e1], s);
+            c->ev_rec.push_back({stage, {e0, e1}});
+        }
+    }
+    int take() {
+        size_t used = 2 * c->ev_rec.size() + (e0 >= 0 ? 1 : 0);
+        while (c->ev_pool.size() <= used) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            c->ev_pool.push_back(e);
+        }
+        return (int)used;
+    }
 };
 
 static gnss_status fail(gnss_ctx *c, gnss_status st, const char *fmt, ...) {
@@ -241,6 +275,7 @@ template <typename T> static gnss_status forward_t(gnss_ctx *c, void *f, cudaStr
     X.p[0] = fld<T>(c->scratch, c->nspec, 0);
     RecipeSet none{};
     const long long nlines = (long long)g.nx * g.ny;
+    c->launches += 3;
     CK(c, launch_zpass<T>(g.nz, -1, F, 1, nlines, g.nz2, T(1), c->tw[2], s));
     CK(c, launch_strided<T>(g.ny, -1, false, F, X, y_strides(c, nb_for<T>(g.ny)), g.nx, 1, g, none, c->tw[1], s));
     CK(c, launch_strided<T>(g.nx, -1, false, X, F, x_fwd_strides(c, nb_for<T>(g.nx)), g.ny, 1, g, none, c->tw[0], s));
@@ -257,6 +292,7 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
     RecipeSet none{};
     const long long nlines = (long long)g.nx * g.ny;
     const T scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
+    c->launches += 3;
     CK(c, launch_strided<T>(g.nx, +1, false, F, X, x_inv_strides(c, nb_for<T>(g.nx)), g.ny, 1, g, none, c->tw[0], s));
     CK(c, launch_strided<T>(g.ny, +1, false, X, F, y_strides(c, nb_for<T>(g.ny)), g.nx, 1, g, none, c->tw[1], s));
     CK(c, launch_zpass<T>(g.nz, +1, F, 1, nlines, g.nz2, scale, c->tw[2], s));
@@ -295,15 +331,35 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
     RecipeSet none{};
     const long long nlines = (long long)g.nx * g.ny;
     const T scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
-    CK(c, launch_strided<T>(g.nx, +1, true, SF, P, x_inv_strides(c, nb_for<T>(g.nx)), g.ny, nphys, g, c->recipes,
-                            c->tw[0], s));
-    CK(c, launch_strided<T>(g.ny, +1, false, P, P, y_strides(c, nb_for<T>(g.ny)), g.nx, nphys, g, none, c->tw[1], s));
-    CK(c, launch_zphys<T>(g.nz, P, nphys, nnl, nlines, g.nz2, scale, (T)c->cfg.alpha, c->tw[2], s));
-    CK(c, launch_strided<T>(g.ny, -1, false, NLs, NLs, y_strides(c, nb_for<T>(g.ny)), g.nx, nnl, g, none, c->tw[1], s));
-    CK(c, launch_strided<T>(g.nx, -1, false, NLs, NLx, x_fwd_strides(c, nb_for<T>(g.nx)), g.ny, nnl, g, none,
-                            c->tw[0], s));
-    k_update<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>(SF, H, NLx, g, uc);
-    LAUNCH_CK(c);
+    {
+        StageTimer t(c, s, 0);
+        CK(c, launch_strided<T>(g.nx, +1, true, SF, P, x_inv_strides(c, nb_for<T>(g.nx)), g.ny, nphys, g,
+                                c->recipes, c->tw[0], s));
+    }
+    {
+        StageTimer t(c, s, 1);
+        CK(c, launch_strided<T>(g.ny, +1, false, P, P, y_strides(c, nb_for<T>(g.ny)), g.nx, nphys, g, none,
+                                c->tw[1], s));
+    }
+    {
+        StageTimer t(c, s, 2);
+        CK(c, launch_zphys<T>(g.nz, P, nphys, nnl, nlines, g.nz2, scale, (T)c->cfg.alpha, c->tw[2], s));
+    }
+    {
+        StageTimer t(c, s, 3);
+        CK(c, launch_strided<T>(g.ny, -1, false, NLs, NLs, y_strides(c, nb_for<T>(g.ny)), g.nx, nnl, g, none,
+                                c->tw[1], s));
+    }
+    {
+        StageTimer t(c, s, 4);
+        CK(c, launch_strided<T>(g.nx, -1, false, NLs, NLx, x_fwd_strides(c, nb_for<T>(g.nx)), g.ny, nnl, g, none,
+                                c->tw[0], s));
+    }
+    {
+        StageTimer t(c, s, 5);
+        k_update<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>(SF, H, NLx, g, uc);
+        LAUNCH_CK(c);
+    }
     return GNSS_OK;
 }
 
@@ -353,6 +409,7 @@ template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields 
     void *sp[5] = {st->u, st->v, st->w, st->s, st->c};
     for (int q = 0; q < 5; ++q) F.p[q] = reinterpret_cast<V2<T> *>(sp[q]);
     const int has_s = st->s != nullptr, has_c = st->c != nullptr;
+    c->launches += 2;
     k_stats_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(F, has_s, has_c, c->g, c->stat_part);
     LAUNCH_CK(c);
     k_stats_final<<<1, STAT_SUMS * 32, 0, s>>>(c->stat_part, STAT_BLOCKS, c->stat_dev);
@@ -388,6 +445,29 @@ const char *gnss_status_string(gnss_status st) {
 }
 
 const char *gnss_last_error(const gnss_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+long long gnss_launch_count(const gnss_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+gnss_status gnss_profile_enable(gnss_ctx *c, int on) {
+    if (!c) return GNSS_ERR_INVALID;
+    c->profiling = on != 0;
+    c->ev_rec.clear();
+    return GNSS_OK;
+}
+
+gnss_status gnss_profile_read(gnss_ctx *c, double *ms, long long *launches) {
+    if (!c || !ms || !launches) return fail(c, GNSS_ERR_INVALID, "null argument");
+    for (int k = 0; k < GNSS_NSTAGES; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    for (auto &r : c->ev_rec) {
+        CK(c, cudaEventSynchronize(c->ev_pool[r.second.second]));
+        float t = 0.f;
+        CK(c, cudaEventElapsedTime(&t, c->ev_pool[r.second.first], c->ev_pool[r.second.second]));
+        ms[r.first] += t;
+        launches[r.first] += 1;
+    }
+    c->ev_rec.clear();
+    return GNSS_OK;
+}
 
 size_t gnss_field_bytes(const gnss_ctx *ctx) { return ctx ? ctx->nspec * ctx->elem : 0; }
 size_t gnss_workspace_bytes(const gnss_ctx *ctx) { return ctx ? ctx->owned_bytes : 0; }
@@ -498,6 +578,7 @@ gnss_status gnss_destroy(gnss_ctx *c) {
     if (c->stat_dev) cudaFree(c->stat_dev);
     if (c->stat_host) cudaFreeHost(c->stat_host);
     if (c->res) cudaFree(c->res);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     delete c;
     return GNSS_OK;
 }
@@ -517,6 +598,7 @@ gnss_status gnss_inverse(gnss_ctx *c, void *f, void *stream) {
 }
 
 template <typename T> static gnss_status dealias_t(gnss_ctx *c, void *f, cudaStream_t s) {
+    c->launches++;
     k_dealias<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>(reinterpret_cast<V2<T> *>(f), c->g);
     LAUNCH_CK(c);
     return GNSS_OK;
@@ -531,6 +613,7 @@ template <typename T>
 static gnss_status vort_t(gnss_ctx *c, const void *u, const void *v, const void *w, void *o1, void *o2, void *o3,
                           cudaStream_t s) {
     using V = V2<T>;
+    c->launches++;
     k_vorticity<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>(
         (const V *)u, (const V *)v, (const V *)w, (V *)o1, (V *)o2, (V *)o3, c->g);
     LAUNCH_CK(c);
@@ -546,6 +629,7 @@ gnss_status gnss_vorticity(gnss_ctx *c, const void *uh, const void *vh, const vo
 template <typename T>
 static gnss_status grad_t(gnss_ctx *c, const void *f, void *x, void *y, void *z, cudaStream_t s) {
     using V = V2<T>;
+    c->launches++;
     k_gradient<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>((const V *)f, (V *)x, (V *)y, (V *)z, c->g);
     LAUNCH_CK(c);
     return GNSS_OK;
@@ -559,6 +643,7 @@ gnss_status gnss_gradient(gnss_ctx *c, const void *fh, void *fx, void *fy, void 
 template <typename T>
 static gnss_status divg_t(gnss_ctx *c, const void *x, const void *y, const void *z, void *o, cudaStream_t s) {
     using V = V2<T>;
+    c->launches++;
     k_divergence<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>((const V *)x, (const V *)y, (const V *)z,
                                                                         (V *)o, c->g);
     LAUNCH_CK(c);
@@ -573,6 +658,7 @@ gnss_status gnss_divergence(gnss_ctx *c, const void *fx, const void *fy, const v
 template <typename T>
 static gnss_status rhs_t(gnss_ctx *c, void *ru, void *rv, void *rw, void *rs, void *rc, cudaStream_t s) {
     using V = V2<T>;
+    c->launches++;
     k_make_rhs<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>((V *)ru, (V *)rv, (V *)rw, (V *)rs, (V *)rc,
                                                                       c->g);
     LAUNCH_CK(c);
@@ -596,6 +682,7 @@ static gnss_status timestep_t(gnss_ctx *c, int euler, const gnss_fields *st, con
     for (int q = 0; q < 5; ++q) {
         if (!f[q]) continue;
         if (!rr[q] || (!euler && !oo[q])) return fail(c, GNSS_ERR_INVALID, "missing rhs field %d", q);
+        c->launches++;
         k_timestep<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>((V *)f[q], (const V *)rr[q],
                                                                           (const V *)oo[q], u.num[q], u.dt, euler,
                                                                           c->g);
@@ -618,6 +705,7 @@ static gnss_status upd_t(gnss_ctx *c, const gnss_fields *r, const gnss_fields *r
     for (int q = 0; q < 5; ++q) {
         if (!rr[q] && !oo[q]) continue;
         if (!rr[q] || !oo[q]) return fail(c, GNSS_ERR_INVALID, "field %d given on one side only", q);
+        c->launches++;
         k_shift_history<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>((V *)rr[q], (V *)oo[q],
                                                                                (long long)c->nspec);
         LAUNCH_CK(c);
@@ -635,6 +723,7 @@ static long long npoints(const gnss_ctx *c) { return (long long)c->g.nx * c->g.n
 template <typename T>
 static gnss_status cross_t(gnss_ctx *c, const void *u, const void *v, const void *w, void *o1, void *o2, void *o3,
                            cudaStream_t s) {
+    c->launches++;
     k_cross<T><<<grid_for(npoints(c), 256), 256, 0, s>>>((const T *)u, (const T *)v, (const T *)w, (T *)o1, (T *)o2,
                                                           (T *)o3, c->g);
     LAUNCH_CK(c);
@@ -650,6 +739,7 @@ gnss_status gnss_cross_product(gnss_ctx *c, const void *u, const void *v, const 
 template <typename T>
 static gnss_status dot_t(gnss_ctx *c, const void *a1, const void *a2, const void *a3, const void *b1, const void *b2,
                          const void *b3, void *o, cudaStream_t s) {
+    c->launches++;
     k_dot<T><<<grid_for(npoints(c), 256), 256, 0, s>>>((const T *)a1, (const T *)a2, (const T *)a3, (const T *)b1,
                                                         (const T *)b2, (const T *)b3, (T *)o, c->g);
     LAUNCH_CK(c);
@@ -666,6 +756,7 @@ template <typename T>
 static gnss_status colloid_t(gnss_ctx *c, const void *u, const void *v, const void *w, const void *cc, const void *cx,
                              const void *cy, const void *cz, const void *sx, const void *sy, const void *sz, void *lap,
                              cudaStream_t s) {
+    c->launches++;
     k_colloid<T><<<grid_for(npoints(c), 256), 256, 0, s>>>(
         (const T *)u, (const T *)v, (const T *)w, (const T *)cc, (const T *)cx, (const T *)cy, (const T *)cz,
         (const T *)sx, (const T *)sy, (const T *)sz, (T *)lap, (T)c->cfg.alpha, c->g);

@@ -84,13 +84,18 @@ _SIGS = {
     "gnss_step": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields), ctypes.c_int, _VP],
     "gnss_stats": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_run_host": [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _VP],
+    "gnss_launch_count": [_VP],
+    "gnss_profile_enable": [_VP, ctypes.c_int],
+    "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
 }
 _RESTYPES = {
     "gnss_field_bytes": ctypes.c_size_t,
     "gnss_workspace_bytes": ctypes.c_size_t,
     "gnss_status_string": ctypes.c_char_p,
     "gnss_last_error": ctypes.c_char_p,
+    "gnss_launch_count": ctypes.c_longlong,
 }
+STAGE_NAMES = ("x_inverse", "y_inverse", "z_physical", "y_forward", "x_forward", "spectral_update")
 
 _lib = None
 
@@ -300,6 +305,19 @@ class Context:
                 else ctypes.cast(stats.data_ptr(), ctypes.POINTER(ctypes.c_double))
         self._ck(self.lib.gnss_run_host(self._h, _host_ptr(host_in), _host_ptr(host_out), int(n_steps),
                                         int(bool(first_euler)), sp, _stream(stream)), "gnss_run_host")
+
+    # -- instrumentation ------------------------------------------------------
+    def launch_count(self) -> int:
+        return int(self.lib.gnss_launch_count(self._h))
+
+    def profile(self, on: bool) -> None:
+        self._ck(self.lib.gnss_profile_enable(self._h, int(bool(on))), "gnss_profile_enable")
+
+    def profile_read(self) -> dict:
+        ms = (ctypes.c_double * len(STAGE_NAMES))()
+        n = (ctypes.c_longlong * len(STAGE_NAMES))()
+        self._ck(self.lib.gnss_profile_read(self._h, ms, n), "gnss_profile_read")
+        return {k: (ms[i], int(n[i])) for i, k in enumerate(STAGE_NAMES)}
 
     # reference spellings
     forwardTransform = forward_transform

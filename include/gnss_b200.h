@@ -151,6 +151,20 @@ gnss_status gnss_stats(gnss_ctx *ctx, const gnss_fields *state, double *out, voi
 gnss_status gnss_run_host(gnss_ctx *ctx, const void *host_state_in, void *host_state_out, int n_steps,
                           int first_euler, double *stats_out, void *stream);
 
+/* Instrumentation (no counterpart in the reference, which only brackets its
+ * loop with cudaProfilerStart/Stop, main.cu:171,249).
+ * gnss_launch_count: kernels this context has launched so far.
+ * gnss_profile_enable: when on, gnss_step records CUDA events around each of
+ * its stages (x inverse, y inverse, z physical, y forward, x forward,
+ * spectral update) on the step's stream.
+ * gnss_profile_read: synchronises, then returns for each stage the summed
+ * device time in ms and the number of launches since profiling was enabled
+ * (arrays of GNSS_NSTAGES entries), and clears the record. */
+#define GNSS_NSTAGES 6
+long long gnss_launch_count(const gnss_ctx *ctx);
+gnss_status gnss_profile_enable(gnss_ctx *ctx, int on);
+gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
+
 #ifdef __cplusplus
 }
 #endif

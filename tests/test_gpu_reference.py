@@ -1,0 +1,102 @@
+"""The CUDA path against the reference's own CUDA code.
+
+1. Against the committed golden vectors (tests/golden, outputs of the
+   unmodified reference solver_ps): full states after 1 and several steps.
+2. Live, where the reference build of oracle/build_ref.sh is present
+   (oracle/_ref/<cfg>/refdrv): the 256^3 two-scalar jet (Re 3000, Sc 0.7 and
+   1.0, noise |k| <= 16, dt 5e-4): relative L2 of every field after one step
+   <= 1e-12, and kinetic energy, dissipation, scalar dissipation and scalar
+   variance within 1e-9 over 200 steps.
+"""
+import json
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from _util import rel_l2, to_dev, to_host
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLD = ROOT / "tests" / "golden"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["g12", "g16", "g16a", "c64"])
+def test_cuda_step_matches_reference_goldens(torch_cuda, case):
+    import gnss_b200 as G
+    from golden.make_golden import _low, initial_state
+    torch = torch_cuda
+    z = np.load(GOLD / f"{case}.npz")
+    m = json.loads(str(z["cfg"]))
+    n, ns = m["n"], m["n_scalars"]
+    f = initial_state(n, ns, m["seed"], m["noise_kmax"])[:3 + ns]
+    with G.Context(n, re=m["re"], sc=m["sc"], sc_c=m["sc_c"], alpha=m["alpha"], dt=m["dt"], n_scalars=ns) as ctx:
+        st = [to_dev(torch, a) for a in f]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        ctx.de_alias(st)
+        for s in range(1, m["steps"] + 1):
+            ctx.solver_ps(st, hi, euler=(s == 1))
+            stats = ctx.stats(st)
+            for i, k in enumerate(G.STAT_NAMES):
+                ref = z["stats"][s][i]
+                assert abs(stats[k] - ref) <= 1e-11 * abs(ref) + 1e-300, (s, k, stats[k], ref)
+            if s in m["dumps"]:
+                got = np.stack([to_host(t) for t in st])
+                tol = 1e-12 if s == 1 else 1e-11
+                if f"state_{s}" in z:
+                    for q in range(3 + ns):
+                        assert rel_l2(got[q], z[f"state_{s}"][q]) < tol
+                        assert rel_l2(to_host(hi[q]), z[f"rhsold_{s}"][q]) < tol
+                else:
+                    full = np.concatenate([got, np.zeros((5 - got.shape[0],) + got.shape[1:], got.dtype)])
+                    lo = _low(full, n)
+                    for q in range(3 + ns):
+                        assert rel_l2(lo[q], z[f"low_{s}"][q]) < tol
+
+
+def _refdrv(cfg):
+    p = ROOT / "oracle" / "_ref" / cfg / "refdrv"
+    if not p.exists():
+        pytest.skip(f"reference build {p} not present (oracle/build_ref.sh)")
+    return p
+
+
+@pytest.mark.gpu
+def test_live_reference_256_two_scalars(torch_cuda):
+    """Config: 256^3, Re 3000, Sc 0.7 / 1.0, noise |k| <= 16, dt 5e-4, 200 steps."""
+    import gnss_b200 as G
+    from golden.make_golden import BUILD, initial_state
+    torch = torch_cuda
+    exe = _refdrv("c256")
+    n, ns, steps = 256, 2, 200
+    b = BUILD["c256"]
+    f = initial_state(n, ns, 0, 16.0)
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        with open(td / "ic.bin", "wb") as fp:
+            for a in f:
+                fp.write(np.ascontiguousarray(a).tobytes())
+        r = subprocess.run([str(exe), "run", str(td / "ic.bin"), str(steps), str(td), "1"], capture_output=True,
+                           text=True, timeout=900)
+        assert r.returncode == 0, r.stderr[-2000:]
+        ref_stats = np.fromfile(td / "stats.bin", dtype=np.float64).reshape(steps + 1, 7)
+        ref1 = np.fromfile(td / "state_1.bin", dtype=np.complex128).reshape(5, n, n, n // 2 + 1)
+    with G.Context(n, re=b["re"], sc=b["sc"], sc_c=b["sc_c"], alpha=b["alpha"], dt=b["dt"], n_scalars=ns) as ctx:
+        st = [to_dev(torch, a) for a in f]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        ctx.de_alias(st)
+        worst = 0.0
+        for s in range(1, steps + 1):
+            ctx.solver_ps(st, hi, euler=(s == 1))
+            if s == 1:
+                for q in range(5):
+                    e = rel_l2(to_host(st[q]), ref1[q])
+                    assert e < 1e-12, (q, e)
+            stats = ctx.stats(st)
+            for k, i in (("ke", 0), ("eps", 2), ("chi_s", 3), ("chi_c", 4), ("var_s", 5), ("var_c", 6)):
+                rel = abs(stats[k] - ref_stats[s][i]) / abs(ref_stats[s][i])
+                worst = max(worst, rel)
+                assert rel < 1e-9, (s, k, stats[k], ref_stats[s][i])
+    print(f"worst statistic deviation over {steps} steps: {worst:.2e}")
