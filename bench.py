@@ -253,7 +253,8 @@ def ours(args):
         l64 = run_leg(G, torch, n, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier)
         ms64 = l64["ms"] if red is None else red(l64["ms"])
         fp64 = {"value": round(ws * pts / (ms64 * 1e-3) / 1e6, 3), "ms_per_step": round(ms64, 4),
-                "mixed_over_fp64": round(ms64 / ms, 3)}
+                "mixed_over_fp64": round(ms64 / ms, 3),
+                "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in l64["profile"].items()}}
     e2e = None
     if not args.no_e2e:
         e = run_e2e(G, torch, n, prec, scheme, args.e2e_calls, dev)

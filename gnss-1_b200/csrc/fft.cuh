@@ -219,6 +219,71 @@ __device__ __forceinline__ void fft_columns(int tid, const V2<T> *tw, GLD gld, S
     }
 }
 
+// ---------------------------------------------------------------- stage 0 in registers
+// Stage 0 (span 1, no twiddles) of a column FFT whose inputs a thread already
+// holds in registers: v[p][r] is element (row jj + r*N/R, column b) of the
+// thread's p-th butterfly, job = tid + p*NT, b = job % NB, jj = job / NB.
+template <typename T, int N, int NB, int NT> struct Stage0 {
+    static constexpr int R = plan_radix(N, 0);
+    static constexpr int M = N / R;
+    static constexpr int NJ = M * NB;
+    static constexpr int PER = (NJ + NT - 1) / NT;
+};
+
+// v[p][r] = LD(row, b) for this thread's stage-0 elements
+template <typename T, int N, int NB, int NT, class LD>
+__device__ __forceinline__ void stage0_gather(int tid, V2<T> (&v)[Stage0<T, N, NB, NT>::PER][Stage0<T, N, NB, NT>::R],
+                                              LD ld) {
+    using S0 = Stage0<T, N, NB, NT>;
+#pragma unroll
+    for (int p = 0; p < S0::PER; ++p) {
+        const int job = tid + p * NT;
+        if ((S0::NJ % NT == 0) || job < S0::NJ) {
+            const int b = job % NB, jj = job / NB;
+#pragma unroll
+            for (int r = 0; r < S0::R; ++r) v[p][r] = ld(jj + r * S0::M, b);
+        }
+    }
+}
+
+// Stage 0 from registers: MUL(value, row, b) is applied to each input
+// element and the stage-0 outputs go through ST(row, b, V) (shared memory,
+// or global memory when the transform has a single stage).
+template <typename T, int N, int SIGN, int NB, int NT, class MUL, class ST>
+__device__ __forceinline__ void stage0_from_regs(int tid,
+                                                 const V2<T> (&v)[Stage0<T, N, NB, NT>::PER][Stage0<T, N, NB, NT>::R],
+                                                 MUL mul, ST st) {
+    using V = V2<T>;
+    using S0 = Stage0<T, N, NB, NT>;
+#pragma unroll
+    for (int p = 0; p < S0::PER; ++p) {
+        const int job = tid + p * NT;
+        if ((S0::NJ % NT == 0) || job < S0::NJ) {
+            const int b = job % NB, jj = job / NB;
+            V w[S0::R];
+#pragma unroll
+            for (int r = 0; r < S0::R; ++r) w[r] = mul(v[p][r], jj + r * S0::M, b);
+            Dft<S0::R, SIGN, V>::run(w);
+#pragma unroll
+            for (int r = 0; r < S0::R; ++r) st(jj * S0::R + r, b, w[r]);
+        }
+    }
+}
+
+// Stages 1 .. NSTG-1 of a column FFT whose stage-0 output is in shared
+// memory (accessor SM); the last stage stores through GST.  Requires a
+// barrier between stage 0's stores and this call.
+template <typename T, int N, int SIGN, int NB, int NT, class SM, class GST, class SYNC>
+__device__ __forceinline__ void fft_rest_stages(int tid, const V2<T> *tw, SM sm, GST gst, SYNC sync) {
+    using V = V2<T>;
+    constexpr int NSTG = plan_nstages(N);
+    if constexpr (NSTG > 1) {
+        fft_mid_stages<T, N, 1, NSTG - 1, SIGN, NB, NT>(tid, tw, sm, sync);
+        fft_stage<T, N, NSTG - 1, SIGN, NB, NT, false>(
+            tid, tw, [&](int row, int b) -> V { return sm(row, b); }, gst, sync);
+    }
+}
+
 // Padded index for one contiguous line in shared memory: one spare element
 // every 8 (double2) or 16 (float2) entries keeps the stride-R stores of the
 // early stages free of bank conflicts.

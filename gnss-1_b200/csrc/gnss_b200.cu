@@ -28,10 +28,22 @@ struct gnss_ctx {
     double *stat_host = nullptr;                  // pinned STAT_SUMS
     void *res = nullptr;                          // resident state + history for gnss_run_host (2 * nf fields)
     size_t owned_bytes = 0;
-    int nphys = 0, nnl = 0;                       // quantities in the physical pass, nonlinear outputs
-    RecipeSet recipes{};
+    // fused step layout (set_recipes): x-inverse outputs P, y-inverse outputs
+    // (the raw quantities of the z pass) Q, physical quantities, products
+    int n_xout = 0, n_raw = 0, n_phys = 0, nnl = 0;
+    // kept box of the spherical truncation and the compact internal layouts:
+    //   P fields [x][kept ky][ncp], Q fields [x][y][ncp], R (in Q) [kept ky][kept kx][ncp]
+    KeepMap kx_keep{}, ky_keep{};
+    int nkz = 0, ncp = 0;
+    size_t p_elems = 0, q_elems = 0;
+    int n_xin = 0;                                // x-inverse inputs (state fields; s twice with alpha)
+    signed char xvar_in[6]{}, xvar_n[6]{}, xvar_mul[6][2]{}, xvar_out[6][2]{};
+    signed char yvar_n[MAXF]{}, yvar_mul[MAXF][2]{}, yvar_out[MAXF][2]{};
+    ZRecipeSet zrec{};
     std::string err;
     long long launches = 0;                       // kernels launched by this context
+    unsigned *d_err = nullptr;                    // device error word set by bounded waits that time out
+    int nsm = 148;                                // SMs of the device
     bool profiling = false;
     std::vector<cudaEvent_t> ev_pool;             // profiling events, reused
     std::vector<std::pair<int, std::pair<int, int>>> ev_rec;   // (stage, (start event, end event))
@@ -106,36 +118,57 @@ static bool size_ok(int n) {
 }
 
 static inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// every device pointer must be aligned to one complex element of the context
+static bool al(const gnss_ctx *c, const void *p) {
+    return p == nullptr || (reinterpret_cast<uintptr_t>(p) % c->elem) == 0;
+}
+static bool al_fields(const gnss_ctx *c, const gnss_fields *f) {
+    return !f || (al(c, f->u) && al(c, f->v) && al(c, f->w) && al(c, f->s) && al(c, f->c));
+}
 static inline int grid_for(long long n, int threads) {
     long long b = (n + threads - 1) / threads;
     long long cap = 148LL * 16;
     return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
-// ============================================================== per-size launchers
-template <typename T, int N> struct Launch {
-    static cudaError_t strided(int sign, bool recipe, const FieldSet<T> &src, const FieldSet<T> &dst,
-                               const Strides &st, int nouter, int nfields, const Geom &g, const RecipeSet &rs,
-                               const void *tw, cudaStream_t s) {
-        using C = StridedCfg<T, N>;
-        dim3 grid((unsigned)(nouter * st.ncolblk), (unsigned)nfields);
-        const V2<T> *t = reinterpret_cast<const V2<T> *>(tw);
-        if (sign < 0) {
-            if (recipe) return go(k_strided<T, N, -1, true>, grid, src, dst, st, g, rs, t, s);
-            return go(k_strided<T, N, -1, false>, grid, src, dst, st, g, rs, t, s);
-        }
-        if (recipe) return go(k_strided<T, N, +1, true>, grid, src, dst, st, g, rs, t, s);
-        return go(k_strided<T, N, +1, false>, grid, src, dst, st, g, rs, t, s);
+// Dynamic shared memory above 48 KB needs an opt-in, and the largest carveout
+// lets several blocks share an SM.
+template <class K> static cudaError_t prep_smem(K kern, int bytes) {
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
     }
-    template <class K>
-    static cudaError_t go(K kern, dim3 grid, const FieldSet<T> &src, const FieldSet<T> &dst, const Strides &st,
-                          const Geom &g, const RecipeSet &rs, const V2<T> *tw, cudaStream_t s) {
-        using C = StridedCfg<T, N>;
-        if (C::SMEM > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-            if (e != cudaSuccess) return e;
-        }
-        kern<<<grid, C::NT, C::SMEM, s>>>(src, dst, st, g, rs, tw);
+    if (bytes > 0)
+        return cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared);
+    return cudaSuccess;
+}
+
+// ============================================================== per-size launchers
+template <class K> static int blocks_per_sm(K kern, int threads, int smem) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        n = 1;
+    }
+    return n < 1 ? 1 : n;
+}
+
+template <typename T, int N> struct Launch {
+    static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
+                            cudaStream_t s) {
+        using C = PassCfg<T, N>;
+        auto kern = sign < 0 ? k_pass<T, N, -1> : k_pass<T, N, +1>;
+        cudaError_t e = prep_smem(kern, C::SMEM);
+        if (e != cudaSuccess) return e;
+        static int per_sm[2] = {0, 0};
+        int &ps = per_sm[sign < 0 ? 0 : 1];
+        if (ps == 0) ps = blocks_per_sm(kern, C::NT, C::SMEM);
+        const long long nitems = (long long)sp.nin * sp.outer.count() * sp.ncolblk;
+        long long grid = (long long)ps * nsm;
+        if (grid > nitems) grid = nitems;
+        kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(P, sp, reinterpret_cast<const V2<T> *>(tw));
         return cudaGetLastError();
     }
     static cudaError_t zpass(int dir, const FieldSet<T> &f, int nfields, long long nlines, int nz2, T scale,
@@ -145,25 +178,40 @@ template <typename T, int N> struct Launch {
         dim3 grid((unsigned)((npairs + ZWARPS - 1) / ZWARPS), (unsigned)nfields);
         const V2<T> *t = reinterpret_cast<const V2<T> *>(tw);
         auto kern = dir < 0 ? k_zpass<T, N, -1> : k_zpass<T, N, +1>;
-        if (C::SMEM > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-            if (e != cudaSuccess) return e;
-        }
+        cudaError_t e = prep_smem(kern, C::SMEM);
+        if (e != cudaSuccess) return e;
         kern<<<grid, ZWARPS * 32, C::SMEM, s>>>(f, nlines, nz2, scale, t);
         return cudaGetLastError();
     }
-    static cudaError_t zphys(const FieldSet<T> &f, int nin, int nout, long long nlines, int nz2, T scale, T alpha,
-                             const void *tw, cudaStream_t s) {
-        const int smem = nin * ZPCfg<T, N>::LEN * (int)sizeof(V2<T>);
-        auto kern = k_zphys<T, N>;
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (e != cudaSuccess) return e;
-        }
-        long long npairs = (nlines + 1) / 2;
-        kern<<<(unsigned)npairs, nin * 32, smem, s>>>(f, nin, nout, nlines, nz2, scale, alpha,
-                                                       reinterpret_cast<const V2<T> *>(tw));
+    template <int NPH, int NRAW>
+    static cudaError_t zphys_n(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
+                               int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
+                               cudaStream_t s) {
+        using C = ZPCfg<T, N>;
+        const int pipe_b = C::pipe_bytes(NPH, NRAW, ncp);
+        const int pipe = pipe_b <= C::SMEM_MAX ? 1 : 0;
+        const int smem = pipe ? pipe_b : C::work_bytes(NPH);
+        auto kern = k_zphys<T, N, NPH, NRAW>;
+        cudaError_t e = prep_smem(kern, smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = blocks_per_sm(kern, NPH * 32, smem);
+        const long long npairs = nlines / 2;
+        long long grid = (long long)per_sm * nsm;
+        if (grid > npairs) grid = npairs;
+        kern<<<(unsigned)grid, NPH * 32, smem, s>>>(f, zr, nout, npairs, ncp, nkz, pipe, scale, alpha, dkz,
+                                                     reinterpret_cast<const V2<T> *>(tw), err);
         return cudaGetLastError();
+    }
+    static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
+                             long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
+                             unsigned *err, int nsm, cudaStream_t s) {
+        if (nph == 9 && nraw == 10)
+            return zphys_n<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+        if (nph == 12 && nraw == 13)
+            return zphys_n<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+        if (nph == 14 && nraw == 14)
+            return zphys_n<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+        return cudaErrorInvalidValue;
     }
 };
 
@@ -186,10 +234,9 @@ template <typename T, int N> struct Launch {
     }
 
 template <typename T>
-static cudaError_t launch_strided(int n, int sign, bool recipe, const FieldSet<T> &src, const FieldSet<T> &dst,
-                                  const Strides &st, int nouter, int nfields, const Geom &g, const RecipeSet &rs,
-                                  const void *tw, cudaStream_t s) {
-    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::strided(sign, recipe, src, dst, st, nouter, nfields, g, rs, tw, s)));
+static cudaError_t launch_pass(int n, int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
+                               cudaStream_t s) {
+    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::pass(sign, P, sp, tw, nsm, s)));
 }
 template <typename T>
 static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfields, long long nlines, int nz2, T scale,
@@ -197,20 +244,21 @@ static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfield
     GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::zpass(dir, f, nfields, nlines, nz2, scale, tw, s)));
 }
 template <typename T>
-static cudaError_t launch_zphys(int n, const FieldSet<T> &f, int nin, int nout, long long nlines, int nz2, T scale,
-                                T alpha, const void *tw, cudaStream_t s) {
-    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::zphys(f, nin, nout, nlines, nz2, scale, alpha, tw, s)));
+static cudaError_t launch_zphys(int n, const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
+                                long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
+                                unsigned *err, int nsm, cudaStream_t s) {
+    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::zphys(f, zr, nph, nraw, nout, nlines, ncp, nkz, scale, alpha, dkz, tw,
+                                                      err, nsm, s)));
 }
-
-template <typename T> static int nb_for(int n) {
+template <typename T> static int pass_nb(int n) {
     switch (n) {
-        case 8: return StridedCfg<T, 8>::NB; case 12: return StridedCfg<T, 12>::NB;
-        case 16: return StridedCfg<T, 16>::NB; case 24: return StridedCfg<T, 24>::NB;
-        case 32: return StridedCfg<T, 32>::NB; case 48: return StridedCfg<T, 48>::NB;
-        case 64: return StridedCfg<T, 64>::NB; case 96: return StridedCfg<T, 96>::NB;
-        case 128: return StridedCfg<T, 128>::NB; case 192: return StridedCfg<T, 192>::NB;
-        case 256: return StridedCfg<T, 256>::NB; case 384: return StridedCfg<T, 384>::NB;
-        default: return StridedCfg<T, 512>::NB;
+        case 8: return PassCfg<T, 8>::NB; case 12: return PassCfg<T, 12>::NB;
+        case 16: return PassCfg<T, 16>::NB; case 24: return PassCfg<T, 24>::NB;
+        case 32: return PassCfg<T, 32>::NB; case 48: return PassCfg<T, 48>::NB;
+        case 64: return PassCfg<T, 64>::NB; case 96: return PassCfg<T, 96>::NB;
+        case 128: return PassCfg<T, 128>::NB; case 192: return PassCfg<T, 192>::NB;
+        case 256: return PassCfg<T, 256>::NB; case 384: return PassCfg<T, 384>::NB;
+        default: return PassCfg<T, 512>::NB;
     }
 }
 
@@ -238,31 +286,122 @@ static gnss_status ensure_scratch(gnss_ctx *c, int nfields) {
     return GNSS_OK;
 }
 
-// Strides of the x pass from the spectral layout [y][x][kz] to [x][y][kz]
-// (inverse) and back (forward), and of the y pass on [x][y][kz].
-static Strides x_inv_strides(const gnss_ctx *c, int nb) {
-    const Geom &g = c->g;
-    Strides s;
-    s.s_row = g.nz2; s.s_out = (long long)g.nx * g.nz2;
-    s.d_row = (long long)g.ny * g.nz2; s.d_out = g.nz2;
-    s.ncols = g.nz2; s.ncolblk = (g.nz2 + nb - 1) / nb;
-    return s;
+// Scratch of the fused step: n_xout P fields, n_raw Q fields (and, for the
+// IF-RK3 scheme, the history after them, full reference-layout fields).
+static size_t step_scratch_elems(const gnss_ctx *c) {
+    size_t e = c->p_elems * (size_t)c->n_xout + c->q_elems * (size_t)c->n_raw;
+    if (c->cfg.scheme == GNSS_SCHEME_RK3IF) e += c->nspec * (size_t)(3 + c->cfg.n_scalars);
+    return e;
 }
-static Strides x_fwd_strides(const gnss_ctx *c, int nb) {
-    const Geom &g = c->g;
-    Strides s;
-    s.s_row = (long long)g.ny * g.nz2; s.s_out = g.nz2;
-    s.d_row = g.nz2; s.d_out = (long long)g.nx * g.nz2;
-    s.ncols = g.nz2; s.ncolblk = (g.nz2 + nb - 1) / nb;
-    return s;
+static gnss_status ensure_scratch_step(gnss_ctx *c) {
+    const size_t need = step_scratch_elems(c);
+    const int nf = (int)((need + c->nspec - 1) / c->nspec);   // in units of full fields
+    return ensure_scratch(c, nf);
 }
-static Strides y_strides(const gnss_ctx *c, int nb) {
+
+// Pass geometries of the full 3D transforms (gnss_forward / gnss_inverse):
+// x passes read / write the spectral layout [y][x][kz] on one side and
+// [x][y][kz] on the other; y passes work on [x][y][kz]; every index kept.
+enum PassKind { X_INV, X_FWD, Y_PASS };
+static KeepMap keep_all(int n) { return KeepMap{n, -1}; }
+
+template <typename T> static PassSpec base_spec(const gnss_ctx *c, int nrow_fft, int nin) {
     const Geom &g = c->g;
-    Strides s;
-    s.s_row = g.nz2; s.s_out = (long long)g.ny * g.nz2;
-    s.d_row = g.nz2; s.d_out = (long long)g.ny * g.nz2;
-    s.ncols = g.nz2; s.ncolblk = (g.nz2 + nb - 1) / nb;
-    return s;
+    PassSpec p{};
+    const int nb = pass_nb<T>(nrow_fft);
+    p.ncols = g.nz2;
+    p.out_ncols = g.nz2;
+    p.ncolblk = (g.nz2 + nb - 1) / nb;
+    p.nin = nin;
+    p.n_col = g.nz;
+    p.dk_col = g.dkz;
+    p.kmax2 = g.kmax2;
+    p.mask = 0;
+    for (int i = 0; i < nin; ++i) {   // default: one plain output per input, same index
+        p.nvar[i] = 1;
+        p.vmul[i][0] = V_ONE;
+        p.vout[i][0] = (signed char)i;
+    }
+    return p;
+}
+
+template <typename T> static PassSpec pass_spec(const gnss_ctx *c, PassKind kind, int nin) {
+    const Geom &g = c->g;
+    const long long nz2 = g.nz2;
+    PassSpec p = base_spec<T>(c, kind == Y_PASS ? g.ny : g.nx, nin);
+    switch (kind) {
+        case X_INV:   // rows = kx, outer = ky: spectral -> [x][y][kz]
+            p.s_row = nz2; p.s_out = (long long)g.nx * nz2; p.d_row = (long long)g.ny * nz2; p.d_out = nz2;
+            p.row_in = p.row_out = keep_all(g.nx); p.outer = keep_all(g.ny);
+            p.n_row = g.nx; p.n_out = g.ny; p.dk_row = g.dkx; p.dk_out = g.dky;
+            break;
+        case X_FWD:   // rows = x, outer = y: [x][y][kz] -> spectral
+            p.s_row = (long long)g.ny * nz2; p.s_out = nz2; p.d_row = nz2; p.d_out = (long long)g.nx * nz2;
+            p.row_in = p.row_out = keep_all(g.nx); p.outer = keep_all(g.ny);
+            p.n_row = g.nx; p.n_out = 0; p.dk_row = g.dkx;
+            break;
+        case Y_PASS:  // rows = ky (or y), outer = x
+            p.s_row = nz2; p.s_out = (long long)g.ny * nz2; p.d_row = nz2; p.d_out = (long long)g.ny * nz2;
+            p.row_in = p.row_out = keep_all(g.ny); p.outer = keep_all(g.nx);
+            p.n_row = g.ny; p.n_out = 0; p.dk_row = g.dky;
+            break;
+    }
+    return p;
+}
+
+// Passes of the fused step on the compact layouts (see gnss_ctx):
+//   X_INV_STEP  state [y][x][kz] (kept kx rows, kept ky, kz < nkz) -> P [x][kyc][ncp]
+//   Y_INV_STEP  P [x][kyc][ncp] (rows = y, kept rows only)          -> Q [x][y][ncp]
+//   Y_FWD_STEP  Q [x][y][ncp]                                      -> P [x][kyc][ncp] (kept ky rows)
+//   X_FWD_STEP  P [x][kyc][ncp] (rows = x, outer = kept ky)        -> R [kyc][kxc][ncp] (kept kx rows)
+enum StepPass { X_INV_STEP, Y_INV_STEP, Y_FWD_STEP, X_FWD_STEP };
+template <typename T> static PassSpec step_spec(const gnss_ctx *c, StepPass kind, int nin) {
+    const Geom &g = c->g;
+    const long long ncp = c->ncp;
+    const int nky = c->ky_keep.count(), nkx = c->kx_keep.count();
+    const bool ypass = kind == Y_INV_STEP || kind == Y_FWD_STEP;
+    PassSpec p = base_spec<T>(c, ypass ? g.ny : g.nx, nin);
+    const int nb = pass_nb<T>(ypass ? g.ny : g.nx);
+    p.ncols = (int)ncp;
+    p.out_ncols = (int)ncp;
+    p.ncolblk = (int)(ncp / nb);
+    switch (kind) {
+        case X_INV_STEP:
+            p.s_row = g.nz2; p.s_out = (long long)g.nx * g.nz2;                 // state, expanded ky
+            p.ncols = c->nkz;
+            p.row_in = c->kx_keep; p.row_in_compact = 0;
+            p.row_out = keep_all(g.nx);
+            p.outer = c->ky_keep; p.outer_in_compact = 0; p.outer_out_compact = 1;
+            p.d_row = (long long)nky * ncp; p.d_out = ncp;
+            p.n_row = g.nx; p.n_out = g.ny; p.dk_row = g.dkx; p.dk_out = g.dky;
+            p.mask = 1;
+            break;
+        case Y_INV_STEP:
+            p.s_row = ncp; p.s_out = (long long)nky * ncp;
+            p.row_in = c->ky_keep; p.row_in_compact = 1;
+            p.row_out = keep_all(g.ny);
+            p.outer = keep_all(g.nx);
+            p.d_row = ncp; p.d_out = (long long)g.ny * ncp;
+            p.n_row = g.ny; p.n_out = 0; p.dk_row = g.dky;
+            break;
+        case Y_FWD_STEP:
+            p.s_row = ncp; p.s_out = (long long)g.ny * ncp;
+            p.row_in = keep_all(g.ny);
+            p.row_out = c->ky_keep; p.row_out_compact = 1;
+            p.outer = keep_all(g.nx);
+            p.d_row = ncp; p.d_out = (long long)nky * ncp;
+            p.n_row = g.ny; p.n_out = 0; p.dk_row = g.dky;
+            break;
+        case X_FWD_STEP:
+            p.s_row = (long long)nky * ncp; p.s_out = ncp;
+            p.row_in = keep_all(g.nx);
+            p.row_out = c->kx_keep; p.row_out_compact = 1;
+            p.outer = c->ky_keep; p.outer_in_compact = 1; p.outer_out_compact = 1;
+            p.d_row = ncp; p.d_out = (long long)nkx * ncp;
+            p.n_row = g.nx; p.n_out = 0; p.dk_row = g.dkx;
+            break;
+    }
+    return p;
 }
 
 // ============================================================== transforms
@@ -270,15 +409,19 @@ template <typename T> static gnss_status forward_t(gnss_ctx *c, void *f, cudaStr
     gnss_status st = ensure_scratch(c, 1);
     if (st) return st;
     const Geom &g = c->g;
-    FieldSet<T> F{}, X{};
+    FieldSet<T> F{};
     F.p[0] = reinterpret_cast<V2<T> *>(f);
-    X.p[0] = fld<T>(c->scratch, c->nspec, 0);
-    RecipeSet none{};
+    V2<T> *X = fld<T>(c->scratch, c->nspec, 0);
     const long long nlines = (long long)g.nx * g.ny;
     c->launches += 3;
     CK(c, launch_zpass<T>(g.nz, -1, F, 1, nlines, g.nz2, T(1), c->tw[2], s));
-    CK(c, launch_strided<T>(g.ny, -1, false, F, X, y_strides(c, nb_for<T>(g.ny)), g.nx, 1, g, none, c->tw[1], s));
-    CK(c, launch_strided<T>(g.nx, -1, false, X, F, x_fwd_strides(c, nb_for<T>(g.nx)), g.ny, 1, g, none, c->tw[0], s));
+    PassPtrs<T> P{};
+    P.in[0] = F.p[0];
+    P.out[0] = X;
+    CK(c, launch_pass<T>(g.ny, -1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s));
+    P.in[0] = X;
+    P.out[0] = F.p[0];
+    CK(c, launch_pass<T>(g.nx, -1, P, pass_spec<T>(c, X_FWD, 1), c->tw[0], c->nsm, s));
     return GNSS_OK;
 }
 
@@ -286,78 +429,102 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
     gnss_status st = ensure_scratch(c, 1);
     if (st) return st;
     const Geom &g = c->g;
-    FieldSet<T> F{}, X{};
+    FieldSet<T> F{};
     F.p[0] = reinterpret_cast<V2<T> *>(f);
-    X.p[0] = fld<T>(c->scratch, c->nspec, 0);
-    RecipeSet none{};
+    V2<T> *X = fld<T>(c->scratch, c->nspec, 0);
     const long long nlines = (long long)g.nx * g.ny;
     const T scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
     c->launches += 3;
-    CK(c, launch_strided<T>(g.nx, +1, false, F, X, x_inv_strides(c, nb_for<T>(g.nx)), g.ny, 1, g, none, c->tw[0], s));
-    CK(c, launch_strided<T>(g.ny, +1, false, X, F, y_strides(c, nb_for<T>(g.ny)), g.nx, 1, g, none, c->tw[1], s));
+    PassPtrs<T> P{};
+    P.in[0] = F.p[0];
+    P.out[0] = X;
+    CK(c, launch_pass<T>(g.nx, +1, P, pass_spec<T>(c, X_INV, 1), c->tw[0], c->nsm, s));
+    P.in[0] = X;
+    P.out[0] = F.p[0];
+    CK(c, launch_pass<T>(g.ny, +1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s));
     CK(c, launch_zpass<T>(g.nz, +1, F, 1, nlines, g.nz2, scale, c->tw[2], s));
     return GNSS_OK;
 }
 
 // ============================================================== fused step
 // One evaluation of the nonlinear term followed by the spectral update.
-//   1 x inverse of the dealiased state, forming u, omega, grad s (, grad c, c, lap s)
-//   2 y inverse of those quantities
-//   3 z C2R + products + z R2C  (physical space stays on chip)
-//   4 y forward of the products
-//   5 x forward of the products into spectral layout
-//   6 projection, dealias and time update
+//   1 x inverse of the dealiased state: X[f] and X[i kx f]                (state -> P)
+//   2 y inverse: Y[.] and Y[i ky .]                                        (P -> Q)
+//   3 z: kz factors and vorticity combinations, C2R, products, R2C        (Q -> Q[0..nnl))
+//      (physical space stays on chip)
+//   4 y forward of the products (in place)                                 (Q)
+//   5 x forward of the products into the spectral layout                   (Q -> P)
+//   6 projection, dealias and time update                                  (P, state, hist)
 template <typename T>
 static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, void *hist_base, const gnss_fields *hist,
                                         const UpdCoef &uc, cudaStream_t s) {
     const Geom &g = c->g;
-    const int nphys = c->nphys, nnl = c->nnl;
-    gnss_status st = ensure_scratch(c, nphys);
+    const int np = c->n_xout, nq = c->n_raw, nnl = c->nnl;
+    gnss_status st = ensure_scratch_step(c);
     if (st) return st;
-    FieldSet<T> SF{}, P{}, NLs{}, NLx{}, H{};
+    V2<T> *Pb = reinterpret_cast<V2<T> *>(c->scratch);
+    V2<T> *Qb = Pb + c->p_elems * (size_t)np;
+    auto Pf = [&](int q) { return Pb + c->p_elems * (size_t)q; };
+    auto Qf = [&](int q) { return Qb + c->q_elems * (size_t)q; };
+    FieldSet<T> SF{}, Q{}, R{}, H{};
     void *sp[5] = {state->u, state->v, state->w, state->s, state->c};
     for (int q = 0; q < 5; ++q) SF.p[q] = reinterpret_cast<V2<T> *>(sp[q]);
-    for (int q = 0; q < nphys; ++q) P.p[q] = fld<T>(c->scratch, c->nspec, q);
-    for (int q = 0; q < nnl; ++q) {
-        NLs.p[q] = P.p[q];
-        NLx.p[q] = P.p[nnl + q];
-    }
+    for (int q = 0; q < nq; ++q) Q.p[q] = Qf(q);
+    for (int q = 0; q < nnl; ++q) R.p[q] = Qf(q);   // x forward output reuses Q storage
     if (hist) {
         void *hp[5] = {hist->u, hist->v, hist->w, hist->s, hist->c};
         for (int q = 0; q < 5; ++q) H.p[q] = reinterpret_cast<V2<T> *>(hp[q]);
     } else {
         for (int q = 0; q < 5; ++q) H.p[q] = fld<T>(hist_base, c->nspec, q);
     }
-    RecipeSet none{};
     const long long nlines = (long long)g.nx * g.ny;
     const T scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
     {
         StageTimer t(c, s, 0);
-        CK(c, launch_strided<T>(g.nx, +1, true, SF, P, x_inv_strides(c, nb_for<T>(g.nx)), g.ny, nphys, g,
-                                c->recipes, c->tw[0], s));
+        PassPtrs<T> P{};
+        const int nxi = c->n_xin;
+        for (int q = 0; q < nxi; ++q) P.in[q] = SF.p[c->xvar_in[q]];
+        for (int q = 0; q < np; ++q) P.out[q] = Pf(q);
+        PassSpec spx = step_spec<T>(c, X_INV_STEP, nxi);
+        for (int i = 0; i < nxi; ++i) {
+            spx.nvar[i] = c->xvar_n[i];
+            for (int v = 0; v < 2; ++v) { spx.vmul[i][v] = c->xvar_mul[i][v]; spx.vout[i][v] = c->xvar_out[i][v]; }
+        }
+        CK(c, launch_pass<T>(g.nx, +1, P, spx, c->tw[0], c->nsm, s));
     }
     {
         StageTimer t(c, s, 1);
-        CK(c, launch_strided<T>(g.ny, +1, false, P, P, y_strides(c, nb_for<T>(g.ny)), g.nx, nphys, g, none,
-                                c->tw[1], s));
+        PassPtrs<T> P{};
+        for (int q = 0; q < np; ++q) P.in[q] = Pf(q);
+        for (int q = 0; q < nq; ++q) P.out[q] = Qf(q);
+        PassSpec spy = step_spec<T>(c, Y_INV_STEP, np);
+        for (int i = 0; i < np; ++i) {
+            spy.nvar[i] = c->yvar_n[i];
+            for (int v = 0; v < 2; ++v) { spy.vmul[i][v] = c->yvar_mul[i][v]; spy.vout[i][v] = c->yvar_out[i][v]; }
+        }
+        CK(c, launch_pass<T>(g.ny, +1, P, spy, c->tw[1], c->nsm, s));
     }
     {
         StageTimer t(c, s, 2);
-        CK(c, launch_zphys<T>(g.nz, P, nphys, nnl, nlines, g.nz2, scale, (T)c->cfg.alpha, c->tw[2], s));
+        CK(c, launch_zphys<T>(g.nz, Q, c->zrec, c->n_phys, nq, nnl, nlines, c->ncp, c->nkz, scale, (T)c->cfg.alpha,
+                              g.dkz, c->tw[2], c->d_err, c->nsm, s));
     }
     {
         StageTimer t(c, s, 3);
-        CK(c, launch_strided<T>(g.ny, -1, false, NLs, NLs, y_strides(c, nb_for<T>(g.ny)), g.nx, nnl, g, none,
-                                c->tw[1], s));
+        PassPtrs<T> P{};
+        for (int q = 0; q < nnl; ++q) { P.in[q] = Qf(q); P.out[q] = Pf(q); }
+        CK(c, launch_pass<T>(g.ny, -1, P, step_spec<T>(c, Y_FWD_STEP, nnl), c->tw[1], c->nsm, s));
     }
     {
         StageTimer t(c, s, 4);
-        CK(c, launch_strided<T>(g.nx, -1, false, NLs, NLx, x_fwd_strides(c, nb_for<T>(g.nx)), g.ny, nnl, g, none,
-                                c->tw[0], s));
+        PassPtrs<T> P{};
+        for (int q = 0; q < nnl; ++q) { P.in[q] = Pf(q); P.out[q] = R.p[q]; }
+        CK(c, launch_pass<T>(g.nx, -1, P, step_spec<T>(c, X_FWD_STEP, nnl), c->tw[0], c->nsm, s));
     }
     {
         StageTimer t(c, s, 5);
-        k_update<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>(SF, H, NLx, g, uc);
+        const long long nmodes = (long long)c->ky_keep.count() * c->kx_keep.count() * c->nkz;
+        k_update<T><<<grid_for(nmodes, 256), 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc);
         LAUNCH_CK(c);
     }
     return GNSS_OK;
@@ -372,7 +539,7 @@ static UpdCoef base_coef(const gnss_ctx *c) {
     // solver.cu:599-611: num = Re for u, v, w; Re*Sc for s; Re*Sc_c for c
     const double num[5] = {k.re, k.re, k.re, k.re * k.sc, k.re * k.sc_c};
     for (int q = 0; q < 5; ++q) {
-        u.num[q] = num[q];
+        u.hnum[q] = k.dt / 2.0 / num[q];
         u.nu[q] = 1.0 / num[q];
     }
     return u;
@@ -386,10 +553,10 @@ static gnss_status step_t(gnss_ctx *c, const gnss_fields *state, const gnss_fiel
         return nonlinear_and_update<T>(c, state, nullptr, hist, uc, s);
     }
     // IF-RK3: the history lives in context scratch after the step's quantities
-    const int nf = 3 + c->cfg.n_scalars;
-    gnss_status st = ensure_scratch(c, c->nphys + nf);
+    gnss_status st = ensure_scratch_step(c);
     if (st) return st;
-    void *hb = fld<T>(c->scratch, c->nspec, c->nphys);
+    void *hb = reinterpret_cast<V2<T> *>(c->scratch) + c->p_elems * (size_t)c->n_xout +
+               c->q_elems * (size_t)c->n_raw;
     const double gam[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
     const double zet[4] = {0.0, -17.0 / 60.0, -5.0 / 12.0, 0.0};
     for (int k = 0; k < 3; ++k) {
@@ -416,6 +583,8 @@ template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields 
     LAUNCH_CK(c);
     CK(c, cudaMemcpyAsync(c->stat_host, c->stat_dev, sizeof(double) * STAT_SUMS, cudaMemcpyDeviceToHost, s));
     CK(c, cudaStreamSynchronize(s));
+    gnss_status chk = gnss_check(c, s);
+    if (chk) return chk;
     const gnss_config &k = c->cfg;
     const double nn = (double)k.nx * k.ny * k.nz;
     const double n2 = nn * nn;
@@ -440,6 +609,7 @@ const char *gnss_status_string(gnss_status st) {
         case GNSS_ERR_CUDA: return "CUDA error";
         case GNSS_ERR_NOMEM: return "out of memory";
         case GNSS_ERR_UNSUPPORTED: return "unsupported";
+        case GNSS_ERR_TIMEOUT: return "device wait timed out";
         default: return "unknown status";
     }
 }
@@ -447,6 +617,20 @@ const char *gnss_status_string(gnss_status st) {
 const char *gnss_last_error(const gnss_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 long long gnss_launch_count(const gnss_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+gnss_status gnss_check(gnss_ctx *c, void *stream) {
+    if (!c) return GNSS_ERR_INVALID;
+    CK(c, cudaSetDevice(c->cfg.device));
+    unsigned h = 0;
+    CK(c, cudaMemcpyAsync(&h, c->d_err, sizeof h, cudaMemcpyDeviceToHost, S(stream)));
+    CK(c, cudaStreamSynchronize(S(stream)));
+    if (h) {
+        CK(c, cudaMemsetAsync(c->d_err, 0, sizeof h, S(stream)));
+        CK(c, cudaStreamSynchronize(S(stream)));
+        return fail(c, GNSS_ERR_TIMEOUT, "a bounded device wait timed out (flags 0x%x)", h);
+    }
+    return GNSS_OK;
+}
 
 gnss_status gnss_profile_enable(gnss_ctx *c, int on) {
     if (!c) return GNSS_ERR_INVALID;
@@ -490,37 +674,111 @@ template <typename T> static void *make_twiddles(int n, gnss_ctx *c) {
     return d;
 }
 
+// Derivatives are split across the passes: kx factors in the x inverse, ky
+// factors in the y inverse, kz factors and the two-field combinations of the
+// vorticity (solver.cu:68-114) in the z pass.
+//   x inverse (state -> P):  P0 X[u] P1 X[v] P2 X[w] P3 X[s] P4 X[ikx v] P5 X[ikx w]
+//                            P6 X[ikx s] [P7 X[c] P8 X[ikx c]] [P9 X[-k^2 s]]
+//   y inverse (P -> Q):      Q0 U00 Q1 V00 Q2 W00 Q3 S00 Q4 U01 Q5 W01 Q6 S01
+//                            Q7 V10 Q8 W10 Q9 S10 [Q10 C00 Q11 C01 Q12 C10] [Q13 L00]
+//   (first index: i kx applied, second: i ky applied)
+//   z pass:  u = U00, v = V00, w = W00, w1 = W01 - ikz V00, w2 = ikz U00 - W10,
+//            w3 = V10 - U01, sx = S10, sy = S01, sz = ikz S00,
+//            [cx = C10, cy = C01, cz = ikz C00], [c = C00, lap s = L00]
 static void set_recipes(gnss_ctx *c) {
-    // state fields: 0 u, 1 v, 2 w, 3 s, 4 c
-    auto R = [](int f0, int m0, int s0, int f1 = -1, int m1 = 0, int s1 = 1) {
-        Recipe r{};
-        r.f[0] = (signed char)f0; r.m[0] = (signed char)m0; r.s[0] = (signed char)s0;
-        r.f[1] = (signed char)f1; r.m[1] = (signed char)m1; r.s[1] = (signed char)s1;
-        return r;
+    const bool two = c->cfg.n_scalars > 1, al = two && c->cfg.alpha != 0.0;
+    auto xv = [&](int in, int var, int mul, int out) {
+        c->xvar_mul[in][var] = (signed char)mul;
+        c->xvar_out[in][var] = (signed char)out;
+        if (c->xvar_n[in] < var + 1) c->xvar_n[in] = (signed char)(var + 1);
     };
-    RecipeSet &rs = c->recipes;
-    int n = 0;
-    rs.r[n++] = R(0, M_ONE, 1);                  // u
-    rs.r[n++] = R(1, M_ONE, 1);                  // v
-    rs.r[n++] = R(2, M_ONE, 1);                  // w
-    rs.r[n++] = R(2, M_IKY, 1, 1, M_IKZ, -1);    // omega_1 = i k2 w - i k3 v   (solver.cu:68-81)
-    rs.r[n++] = R(0, M_IKZ, 1, 2, M_IKX, -1);    // omega_2 = i k3 u - i k1 w   (solver.cu:84-97)
-    rs.r[n++] = R(1, M_IKX, 1, 0, M_IKY, -1);    // omega_3 = i k1 v - i k2 u   (solver.cu:100-113)
-    rs.r[n++] = R(3, M_IKX, 1);                  // ds/dx  (gradientKernel_mgpu, solver.cu:233-256)
-    rs.r[n++] = R(3, M_IKY, 1);
-    rs.r[n++] = R(3, M_IKZ, 1);
-    c->nnl = 4;
-    if (c->cfg.n_scalars > 1) {
-        rs.r[n++] = R(4, M_IKX, 1);              // grad c (solver.cu:444)
-        rs.r[n++] = R(4, M_IKY, 1);
-        rs.r[n++] = R(4, M_IKZ, 1);
-        c->nnl = 5;
-        if (c->cfg.alpha != 0.0) {
-            rs.r[n++] = R(4, M_ONE, 1);          // c itself (solver.cu:451)
-            rs.r[n++] = R(3, M_LAP, 1);          // lap s = div grad s (solver.cu:425)
+    for (int i = 0; i < 5; ++i) c->xvar_in[i] = (signed char)i;
+    xv(0, 0, V_ONE, 0);
+    xv(1, 0, V_ONE, 1); xv(1, 1, V_IK_ROW, 4);
+    xv(2, 0, V_ONE, 2); xv(2, 1, V_IK_ROW, 5);
+    xv(3, 0, V_ONE, 3); xv(3, 1, V_IK_ROW, 6);
+    c->n_xin = 4;
+    c->n_xout = 7;
+    if (two) {
+        xv(4, 0, V_ONE, 7); xv(4, 1, V_IK_ROW, 8);
+        c->n_xin = 5;
+        c->n_xout = 9;
+        if (al) {   // s a second time, for -k^2 s
+            c->xvar_in[5] = 3;
+            xv(5, 0, V_LAP, 9);
+            c->n_xin = 6;
+            c->n_xout = 10;
         }
     }
-    c->nphys = n;
+    auto yv = [&](int in, int var, int mul, int out) {
+        c->yvar_mul[in][var] = (signed char)mul;
+        c->yvar_out[in][var] = (signed char)out;
+        if (c->yvar_n[in] < var + 1) c->yvar_n[in] = (signed char)(var + 1);
+    };
+    yv(0, 0, V_ONE, 0); yv(0, 1, V_IK_ROW, 4);    // X[u]     -> U00, U01
+    yv(1, 0, V_ONE, 1);                           // X[v]     -> V00
+    yv(2, 0, V_ONE, 2); yv(2, 1, V_IK_ROW, 5);    // X[w]     -> W00, W01
+    yv(3, 0, V_ONE, 3); yv(3, 1, V_IK_ROW, 6);    // X[s]     -> S00, S01
+    yv(4, 0, V_ONE, 7);                           // X[ikx v] -> V10
+    yv(5, 0, V_ONE, 8);                           // X[ikx w] -> W10
+    yv(6, 0, V_ONE, 9);                           // X[ikx s] -> S10
+    c->n_raw = 10;
+    if (two) {
+        yv(7, 0, V_ONE, 10); yv(7, 1, V_IK_ROW, 11);   // X[c]     -> C00, C01
+        yv(8, 0, V_ONE, 12);                           // X[ikx c] -> C10
+        c->n_raw = 13;
+        if (al) { yv(9, 0, V_ONE, 13); c->n_raw = 14; }   // X[-k^2 s] -> L00
+    }
+    auto zq = [&](int q, int r0, int k0, int s0, int r1 = -1, int k1 = 0, int s1 = 1) {
+        ZRecipe &z = c->zrec.q[q];
+        z.r[0] = (signed char)r0; z.ikz[0] = (signed char)k0; z.sgn[0] = (signed char)s0;
+        z.r[1] = (signed char)r1; z.ikz[1] = (signed char)k1; z.sgn[1] = (signed char)s1;
+    };
+    zq(0, 0, 0, 1);               // u
+    zq(1, 1, 0, 1);               // v
+    zq(2, 2, 0, 1);               // w
+    zq(3, 5, 0, 1, 1, 1, -1);     // w1 = W01 - ikz V00
+    zq(4, 0, 1, 1, 8, 0, -1);     // w2 = ikz U00 - W10
+    zq(5, 7, 0, 1, 4, 0, -1);     // w3 = V10 - U01
+    zq(6, 9, 0, 1);               // sx
+    zq(7, 6, 0, 1);               // sy
+    zq(8, 3, 1, 1);               // sz
+    c->n_phys = 9;
+    c->nnl = 4;
+    if (two) {
+        zq(9, 12, 0, 1);          // cx
+        zq(10, 11, 0, 1);         // cy
+        zq(11, 10, 1, 1);         // cz
+        c->n_phys = 12;
+        c->nnl = 5;
+        if (al) {
+            zq(12, 10, 0, 1);     // c
+            zq(13, 13, 0, 1);     // lap s
+            c->n_phys = 14;
+        }
+    }
+}
+
+// Kept indices of one axis: i is kept when its wavenumber alone does not
+// exceed the truncation radius (the test of solver.cu:36 restricted to one
+// axis); with the Nyquist index kept, every index is.
+static KeepMap keep_of(int n, double dk, double kmax2) {
+    const double kn = dk * ((double)(n / 2) - (double)n);
+    if (kn * kn <= kmax2) return KeepMap{n, -1};
+    int K = 0;
+    while (K + 1 < n / 2 && (dk * (double)(K + 1)) * (dk * (double)(K + 1)) <= kmax2) ++K;
+    return KeepMap{n, K};
+}
+
+static void set_layout(gnss_ctx *c) {
+    const Geom &g = c->g;
+    c->kx_keep = keep_of(g.nx, g.dkx, g.kmax2);
+    c->ky_keep = keep_of(g.ny, g.dky, g.kmax2);
+    const KeepMap kz = keep_of(g.nz, g.dkz, g.kmax2);
+    c->nkz = kz.K < 0 ? g.nz2 : kz.K + 1;
+    c->ncp = (c->nkz + 15) / 16 * 16;
+    c->p_elems = (size_t)g.nx * c->ky_keep.count() * c->ncp;
+    c->q_elems = (size_t)g.nx * g.ny * c->ncp;
 }
 
 gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out) {
@@ -552,6 +810,7 @@ gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out) {
     c->nspec = (size_t)k.nx * k.ny * g.nz2;
     c->elem = k.precision == GNSS_FP64 ? sizeof(double2) : sizeof(float2);
     set_recipes(c);
+    set_layout(c);
     const int ns[3] = {k.nx, k.ny, k.nz};
     for (int a = 0; a < 3; ++a) {
         c->tw[a] = k.precision == GNSS_FP64 ? make_twiddles<double>(ns[a], c) : make_twiddles<float>(ns[a], c);
@@ -565,6 +824,12 @@ gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out) {
         return GNSS_ERR_NOMEM;
     }
     c->owned_bytes += sizeof(double) * (STAT_BLOCKS * STAT_SUMS + STAT_SUMS);
+    if (cudaMalloc(&c->d_err, sizeof(unsigned)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        gnss_destroy(c);
+        return GNSS_ERR_NOMEM;
+    }
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, k.device);
     *out = c;
     return GNSS_OK;
 }
@@ -577,6 +842,7 @@ gnss_status gnss_destroy(gnss_ctx *c) {
     if (c->stat_part) cudaFree(c->stat_part);
     if (c->stat_dev) cudaFree(c->stat_dev);
     if (c->stat_host) cudaFreeHost(c->stat_host);
+    if (c->d_err) cudaFree(c->d_err);
     if (c->res) cudaFree(c->res);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     delete c;
@@ -587,12 +853,14 @@ gnss_status gnss_destroy(gnss_ctx *c) {
 
 gnss_status gnss_forward(gnss_ctx *c, void *f, void *stream) {
     if (!c || !f) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, f)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, forward_t, c, f, S(stream));
 }
 
 gnss_status gnss_inverse(gnss_ctx *c, void *f, void *stream) {
     if (!c || !f) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, f)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, inverse_t, c, f, S(stream));
 }
@@ -605,6 +873,7 @@ template <typename T> static gnss_status dealias_t(gnss_ctx *c, void *f, cudaStr
 }
 gnss_status gnss_dealias(gnss_ctx *c, void *f, void *stream) {
     if (!c || !f) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, f)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, dealias_t, c, f, S(stream));
 }
@@ -622,6 +891,7 @@ static gnss_status vort_t(gnss_ctx *c, const void *u, const void *v, const void 
 gnss_status gnss_vorticity(gnss_ctx *c, const void *uh, const void *vh, const void *wh, void *o1, void *o2, void *o3,
                            void *stream) {
     if (!c || !uh || !vh || !wh || !o1 || !o2 || !o3) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, uh) || !al(c, vh) || !al(c, wh) || !al(c, o1) || !al(c, o2) || !al(c, o3)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, vort_t, c, uh, vh, wh, o1, o2, o3, S(stream));
 }
@@ -636,6 +906,7 @@ static gnss_status grad_t(gnss_ctx *c, const void *f, void *x, void *y, void *z,
 }
 gnss_status gnss_gradient(gnss_ctx *c, const void *fh, void *fx, void *fy, void *fz, void *stream) {
     if (!c || !fh || !fx || !fy || !fz) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, fh) || !al(c, fx) || !al(c, fy) || !al(c, fz)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, grad_t, c, fh, fx, fy, fz, S(stream));
 }
@@ -651,6 +922,7 @@ static gnss_status divg_t(gnss_ctx *c, const void *x, const void *y, const void 
 }
 gnss_status gnss_divergence(gnss_ctx *c, const void *fx, const void *fy, const void *fz, void *out, void *stream) {
     if (!c || !fx || !fy || !fz || !out) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, fx) || !al(c, fy) || !al(c, fz) || !al(c, out)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, divg_t, c, fx, fy, fz, out, S(stream));
 }
@@ -666,6 +938,7 @@ static gnss_status rhs_t(gnss_ctx *c, void *ru, void *rv, void *rw, void *rs, vo
 }
 gnss_status gnss_make_rhs(gnss_ctx *c, void *ru, void *rv, void *rw, void *rs, void *rc, void *stream) {
     if (!c || !ru || !rv || !rw) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, ru) || !al(c, rv) || !al(c, rw) || !al(c, rs) || !al(c, rc)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, rhs_t, c, ru, rv, rw, rs, rc, S(stream));
 }
@@ -675,6 +948,8 @@ static gnss_status timestep_t(gnss_ctx *c, int euler, const gnss_fields *st, con
                               const gnss_fields *ro, cudaStream_t s) {
     using V = V2<T>;
     UpdCoef u = base_coef(c);
+    const gnss_config &k = c->cfg;
+    const double num[5] = {k.re, k.re, k.re, k.re * k.sc, k.re * k.sc_c};   // solver.cu:599-611
     void *f[5] = {st->u, st->v, st->w, st->s, st->c};
     void *rr[5] = {r->u, r->v, r->w, r->s, r->c};
     void *oo[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -684,7 +959,7 @@ static gnss_status timestep_t(gnss_ctx *c, int euler, const gnss_fields *st, con
         if (!rr[q] || (!euler && !oo[q])) return fail(c, GNSS_ERR_INVALID, "missing rhs field %d", q);
         c->launches++;
         k_timestep<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>((V *)f[q], (const V *)rr[q],
-                                                                          (const V *)oo[q], u.num[q], u.dt, euler,
+                                                                          (const V *)oo[q], num[q], u.dt, euler,
                                                                           c->g);
         LAUNCH_CK(c);
     }
@@ -693,6 +968,8 @@ static gnss_status timestep_t(gnss_ctx *c, int euler, const gnss_fields *st, con
 gnss_status gnss_timestep(gnss_ctx *c, int euler, const gnss_fields *state, const gnss_fields *rhs,
                           const gnss_fields *rhs_old, void *stream) {
     if (!c || !state || !rhs || (!euler && !rhs_old)) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al_fields(c, state) || !al_fields(c, rhs) || !al_fields(c, rhs_old))
+        return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, timestep_t, c, euler, state, rhs, rhs_old, S(stream));
 }
@@ -714,6 +991,7 @@ static gnss_status upd_t(gnss_ctx *c, const gnss_fields *r, const gnss_fields *r
 }
 gnss_status gnss_update(gnss_ctx *c, const gnss_fields *rhs, const gnss_fields *rhs_old, void *stream) {
     if (!c || !rhs || !rhs_old) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al_fields(c, rhs) || !al_fields(c, rhs_old)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, upd_t, c, rhs, rhs_old, S(stream));
 }
@@ -732,6 +1010,7 @@ static gnss_status cross_t(gnss_ctx *c, const void *u, const void *v, const void
 gnss_status gnss_cross_product(gnss_ctx *c, const void *u, const void *v, const void *w, void *o1, void *o2, void *o3,
                                void *stream) {
     if (!c || !u || !v || !w || !o1 || !o2 || !o3) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, u) || !al(c, v) || !al(c, w) || !al(c, o1) || !al(c, o2) || !al(c, o3)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, cross_t, c, u, v, w, o1, o2, o3, S(stream));
 }
@@ -748,6 +1027,7 @@ static gnss_status dot_t(gnss_ctx *c, const void *a1, const void *a2, const void
 gnss_status gnss_dot_product(gnss_ctx *c, const void *a1, const void *a2, const void *a3, const void *b1,
                              const void *b2, const void *b3, void *out, void *stream) {
     if (!c || !a1 || !a2 || !a3 || !b1 || !b2 || !b3 || !out) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, a1) || !al(c, a2) || !al(c, a3) || !al(c, b1) || !al(c, b2) || !al(c, b3) || !al(c, out)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, dot_t, c, a1, a2, a3, b1, b2, b3, out, S(stream));
 }
@@ -768,6 +1048,7 @@ gnss_status gnss_colloid_advection(gnss_ctx *c, const void *u, const void *v, co
                                    const void *sz, void *lap_s_inout, void *stream) {
     if (!c || !u || !v || !w || !cc || !cx || !cy || !cz || !sx || !sy || !sz || !lap_s_inout)
         return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al(c, u) || !al(c, v) || !al(c, w) || !al(c, cc) || !al(c, cx) || !al(c, cy) || !al(c, cz) || !al(c, sx) || !al(c, sy) || !al(c, sz) || !al(c, lap_s_inout)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, colloid_t, c, u, v, w, cc, cx, cy, cz, sx, sy, sz, lap_s_inout, S(stream));
 }
@@ -783,6 +1064,7 @@ gnss_status gnss_step(gnss_ctx *c, const gnss_fields *state, const gnss_fields *
     if (!state_ok(c, state)) return fail(c, GNSS_ERR_INVALID, "state fields missing");
     if (c->cfg.scheme == GNSS_SCHEME_CNAB2 && !state_ok(c, hist))
         return fail(c, GNSS_ERR_INVALID, "history fields missing");
+    if (!al_fields(c, state) || !al_fields(c, hist)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, step_t, c, state, hist, euler, S(stream));
 }
@@ -790,6 +1072,7 @@ gnss_status gnss_step(gnss_ctx *c, const gnss_fields *state, const gnss_fields *
 gnss_status gnss_stats(gnss_ctx *c, const gnss_fields *state, double *out, void *stream) {
     if (!c || !out) return fail(c, GNSS_ERR_INVALID, "null argument");
     if (!state || !state->u || !state->v || !state->w) return fail(c, GNSS_ERR_INVALID, "state fields missing");
+    if (!al_fields(c, state)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, stats_t, c, state, out, S(stream));
 }
@@ -819,6 +1102,10 @@ gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int 
     }
     CK(c, cudaMemcpyAsync(base, host_in, (size_t)nf * fb, cudaMemcpyHostToDevice, s));
     CK(c, cudaMemsetAsync(base + (size_t)nf * fb, 0, (size_t)nf * fb, s));
+    for (int q = 0; q < nf; ++q) {   // as the reference does before its loop (main.cu:156)
+        gnss_status r = gnss_dealias(c, *sp[q], stream);
+        if (r) return r;
+    }
     for (int i = 0; i < n_steps; ++i) {
         gnss_status r = gnss_step(c, &st, &hi, (i == 0 && first_euler) ? 1 : 0, stream);
         if (r) return r;
@@ -829,6 +1116,6 @@ gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int 
     }
     CK(c, cudaMemcpyAsync(host_out, base, (size_t)nf * fb, cudaMemcpyDeviceToHost, s));
     CK(c, cudaStreamSynchronize(s));
-    return GNSS_OK;
+    return gnss_check(c, stream);
 }
 

@@ -1,8 +1,10 @@
 // kernels.cuh -- the B200 kernels of the pseudospectral step.
 //
-//   k_strided   x / y axis C2C pass over [outer][row][col] tiles, optionally
-//               transposed on store, optionally forming ik-derivative
-//               combinations of the dealiased state on load (x inverse).
+//   k_pass      x / y axis C2C pass over [outer][row][col] tiles, persistent
+//               and software-pipelined (cp.async double buffering); every
+//               input tile is read once and may yield two outputs with
+//               different spectral multipliers (derivatives), optionally
+//               dealiased, optionally transposed on store.
 //   k_zpass     z axis R2C / C2R over pairs of contiguous lines (a + ib).
 //   k_zphys     fused z C2R of all physical quantities of a line pair, the
 //               nonlinear products (omega x u, u.grad s, colloid term) and the
@@ -12,6 +14,7 @@
 //   k_stats_*   deterministic compensated statistics reductions.
 //   elementwise kernels mirroring the reference's individual operators.
 #pragma once
+#include "async.cuh"
 #include "fft.cuh"
 
 namespace gnss {
@@ -35,89 +38,170 @@ __device__ __forceinline__ double ksq3(double a, double b, double c) {
     return __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
 }
 
-// ------------------------------------------------------------ recipes
-// A recipe builds one spectral quantity from at most two state fields:
-// out = sum_t sign_t * M_t(k) * state[f_t], M in {1, i kx, i ky, i kz, -k^2}.
-enum : signed char { M_ONE = 0, M_IKX = 1, M_IKY = 2, M_IKZ = 3, M_LAP = 4 };
-struct Recipe { signed char f[2]; signed char m[2]; signed char s[2]; signed char pad[2]; };
-struct RecipeSet { Recipe r[MAXF]; };
+// ------------------------------------------------------------ strided pass
+// A pass transforms along one axis of a field viewed as [outer][row][col]
+// (row = the transform index, col = the contiguous kz index).  Work items are
+// (input field, tile) with a tile of NB columns x N rows, rows of 128 bytes.
+// Every input tile is read from HBM once and may produce up to two outputs,
+// each the transform of the tile times a spectral multiplier:
+//   V_ONE 1, V_IK_ROW i k_row, V_IK_OUT i k_outer, V_IK_COL i k_col,
+//   V_LAP -(k_row^2 + k_outer^2 + k_col^2),
+// optionally after the dealias mask k^2 > kmax^2 -> 0 (all three wavenumbers
+// are known in the first, spectral-side pass).  Outputs are written with
+// their own strides (a transposed store for the x passes).
+enum : signed char { V_ONE = 0, V_IK_ROW = 1, V_IK_OUT = 2, V_IK_COL = 3, V_LAP = 4 };
 
-template <typename V> __device__ __forceinline__ V apply_mult(V a, int m, double kx, double ky, double kz, double k2) {
-    using T = decltype(a.x);
-    switch (m) {
-        case M_IKX: return V{(T)(-kx) * a.y, (T)kx * a.x};
-        case M_IKY: return V{(T)(-ky) * a.y, (T)ky * a.x};
-        case M_IKZ: return V{(T)(-kz) * a.y, (T)kz * a.x};
-        case M_LAP: return V{(T)(-k2) * a.x, (T)(-k2) * a.y};
-        default: return a;
+// Kept indices of one axis under the spherical truncation: {0..K} and
+// {n-K..n-1}; K < 0 keeps every index.  Compact storage numbers the kept
+// indices 0..2K in order.
+struct KeepMap {
+    int n, K;
+    __host__ __device__ __forceinline__ bool kept(int i) const { return K < 0 || i <= K || i >= n - K; }
+    __host__ __device__ __forceinline__ int compact(int i) const { return (K < 0 || i <= K) ? i : i - (n - 2 * K - 1); }
+    __host__ __device__ __forceinline__ int expand(int c) const { return (K < 0 || c <= K) ? c : c + (n - 2 * K - 1); }
+    __host__ __device__ __forceinline__ int count() const { return K < 0 ? n : 2 * K + 1; }
+};
+
+struct PassSpec {
+    long long s_row, s_out;    // source strides (elements) of row and outer index
+    long long d_row, d_out;    // destination strides
+    KeepMap row_in;            // rows loaded (the others are zero)
+    int row_in_compact;        // loaded rows addressed by their compact index
+    KeepMap row_out;           // rows stored
+    int row_out_compact;       // stored rows addressed by their compact index
+    KeepMap outer;             // outer indices visited (compact enumeration)
+    int outer_in_compact;      // source outer index compact (else the expanded index)
+    int outer_out_compact;     // destination outer index compact
+    int ncols;                 // valid source columns (the others read as zero)
+    int out_ncols;             // destination columns stored
+    int ncolblk;               // column blocks per outer index
+    int nin;                   // input fields; work items = nin * outer.count() * ncolblk
+    int n_row, n_out, n_col;   // axis lengths for the wavenumbers (n_out = 0: outer is physical)
+    double dk_row, dk_out, dk_col;
+    double kmax2;
+    int mask;                  // apply the dealias mask on load
+    signed char nvar[MAXF];    // outputs per input (1 or 2)
+    signed char vmul[MAXF][2]; // multiplier of each output
+    signed char vout[MAXF][2]; // output field index of each output
+};
+template <typename T> struct PassPtrs {
+    const V2<T> *in[MAXF];
+    V2<T> *out[MAXF];
+};
+
+__host__ __device__ constexpr int pow2_floor(int v) {
+    int p = 1;
+    while (p * 2 <= v) p *= 2;
+    return p;
+}
+
+// NB columns of 8 (FP64) or 16 (FP32) complex values make 128-byte rows;
+// each thread owns E complex values of the tile; two staging buffers (the
+// copy pipeline) and one buffer to transform in use at most 192 KB.
+template <typename T, int N> struct PassCfg {
+    static constexpr int ELEM = (int)sizeof(V2<T>);
+    static constexpr int NB0 = (64 * 1024 / ELEM) / N;
+    static constexpr int NB = pow2_floor(NB0 > 16 ? 16 : (NB0 < 1 ? 1 : NB0));
+    static constexpr int E = (sizeof(T) == 8) ? 8 : 16;
+    static constexpr int NT0 = N * NB / E;
+    static constexpr int NT = NT0 < 32 ? 32 : (NT0 > 1024 ? 1024 : NT0);
+    static constexpr int TILE = N * NB;
+    static constexpr bool WORK = plan_nstages(N) > 1;
+    static constexpr int SMEM = (2 + (WORK ? 1 : 0)) * TILE * ELEM;
+};
+
+// Asynchronous copy of one tile (rows kept by row_in, columns < ncols; the
+// rest zero-filled) into shared memory, laid out [row][NB].
+template <typename T>
+__device__ __forceinline__ void tile_prefetch(V2<T> *dst, const V2<T> *__restrict__ src, const PassSpec &sp, int tile,
+                                              int nb, int c0, int tid, int nt) {
+    for (int e = tid; e < tile; e += nt) {
+        const int row = e / nb, b = e % nb;
+        const bool ok = (c0 + b < sp.ncols) && sp.row_in.kept(row);
+        const int r = ok ? (sp.row_in_compact ? sp.row_in.compact(row) : row) : 0;
+        const V2<T> *p = src + (ok ? (long long)r * sp.s_row + b : 0);
+        if constexpr (sizeof(T) == 8) cp_async16(dst + e, p, ok ? 16 : 0);
+        else cp_async8(dst + e, p, ok ? 8 : 0);
     }
 }
 
-// ------------------------------------------------------------ strided pass
-struct Strides {
-    long long s_row, s_out;   // source element strides of the transform index and the outer index
-    long long d_row, d_out;   // destination strides (transposed store when they differ)
-    int ncols;                // contiguous columns per row (nz2)
-    int ncolblk;              // ceil(ncols / NB)
-};
-
-template <typename T, int N> struct StridedCfg {
-    static constexpr int NB = (sizeof(T) == 8) ? ((N >= 512) ? 8 : 16) : 16;
-    static constexpr int NT0 = N * NB / 16;
-    static constexpr int NT = NT0 < 32 ? 32 : (NT0 > 512 ? 512 : NT0);
-    static constexpr int SMEM = (plan_nstages(N) > 1) ? N * NB * (int)sizeof(V2<T>) : 0;
-};
-
-// grid: x = outer * ncolblk + colblk, y = field (or recipe) index.
-// LOAD_RECIPE: row = kx index, outer = ky index, col = kz index of the
-// spectral state in src.p[0..4]; recipe blockIdx.y selects the combination.
-template <typename T, int N, int SIGN, bool RECIPE>
-__global__ void __launch_bounds__(StridedCfg<T, N>::NT)
-k_strided(FieldSet<T> src, FieldSet<T> dst, Strides st, Geom g, RecipeSet rs, const V2<T> *__restrict__ tw) {
+// Persistent: block b handles items b, b + gridDim.x, ... and prefetches the
+// next item's tile while transforming the current one.
+template <typename T, int N, int SIGN>
+__global__ void __launch_bounds__(PassCfg<T, N>::NT, 1)
+k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec sp, const V2<T> *__restrict__ tw) {
     using V = V2<T>;
-    using C = StridedCfg<T, N>;
-    constexpr int NB = C::NB, NT = C::NT;
+    using C = PassCfg<T, N>;
+    constexpr int NB = C::NB, NT = C::NT, TILE = C::TILE;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *sm = reinterpret_cast<V *>(smem_raw);
+    V *rawb[2] = {reinterpret_cast<V *>(smem_raw), reinterpret_cast<V *>(smem_raw) + TILE};
+    V *work = reinterpret_cast<V *>(smem_raw) + 2 * TILE;
     const int tid = threadIdx.x;
-    const int o = blockIdx.x / st.ncolblk;
-    const int c0 = (blockIdx.x % st.ncolblk) * NB;
-    const int f = blockIdx.y;
-    const V *__restrict__ s = src.p[f];
-    V *__restrict__ d = dst.p[f];
-    const long long sbase = (long long)o * st.s_out + c0;
-    const long long dbase = (long long)o * st.d_out + c0;
-    const int ncols = st.ncols;
-
-    auto gld = [&](int row, int b) -> V {
-        const int col = c0 + b;
-        if (col >= ncols) return V{T(0), T(0)};
-        const long long idx = sbase + (long long)row * st.s_row + b;
-        if constexpr (!RECIPE) {
-            return s[idx];
-        } else {
-            const Recipe rc = rs.r[f];
-            const double kx = wavenum(row, g.nx, g.dkx);
-            const double ky = wavenum(o, g.ny, g.dky);
-            const double kz = wavenum(col, g.nz, g.dkz);
-            const double k2 = ksq3(kx, ky, kz);
-            V acc = V{T(0), T(0)};
-            if (k2 > g.kmax2) return acc;   // dealias mask (solver.cu:36)
-#pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                if (rc.f[t] >= 0) {
-                    V a = apply_mult(src.p[rc.f[t]][idx], rc.m[t], kx, ky, kz, k2);
-                    acc = rc.s[t] > 0 ? cadd(acc, a) : csub(acc, a);
+    const int ntiles = sp.outer.count() * sp.ncolblk;
+    const long long nitems = (long long)sp.nin * ntiles;
+    long long item = blockIdx.x;
+    if (item >= nitems) return;
+    // oc: compact outer index, o: expanded outer index
+    auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
+        fi = (int)(it / ntiles);
+        const int t = (int)(it % ntiles);
+        oc = t / sp.ncolblk;
+        o = sp.outer.expand(oc);
+        c0 = (t % sp.ncolblk) * NB;
+    };
+    auto prefetch = [&](long long it, V *dst) {
+        int fi, oc, o, c0;
+        decode(it, fi, oc, o, c0);
+        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        tile_prefetch<T>(dst, src, sp, TILE, NB, c0, tid, NT);
+    };
+    prefetch(item, rawb[0]);
+    cp_async_commit();
+    int buf = 0;
+    for (; item < nitems; item += gridDim.x) {
+        const long long next = item + gridDim.x;
+        if (next < nitems) prefetch(next, rawb[buf ^ 1]);
+        cp_async_commit();
+        cp_async_wait<1>();   // this thread's copies of the current tile have landed
+        __syncthreads();      // ... and everybody else's
+        int fi, oc, o, c0;
+        decode(item, fi, oc, o, c0);
+        const V *cur = rawb[buf];
+        const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
+        const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const int out_cols = sp.out_ncols - c0;
+        const int nv = sp.nvar[fi];
+        for (int v = 0; v < nv; ++v) {
+            const int mul = sp.vmul[fi][v];
+            V *dst = P.out[sp.vout[fi][v]] + dbase;
+            auto gld = [&](int row, int b) -> V {
+                V a = cur[row * NB + b];
+                if (mul == V_ONE && !sp.mask) return a;
+                const double kr = wavenum(row, sp.n_row, sp.dk_row);
+                const double kc = wavenum(c0 + b, sp.n_col, sp.dk_col);
+                const double k2 = ksq3(kr, k_out, kc);
+                if (sp.mask && k2 > sp.kmax2) return V{T(0), T(0)};   // dealias mask (solver.cu:36)
+                switch (mul) {
+                    case V_IK_ROW: return V{(T)(-kr) * a.y, (T)kr * a.x};
+                    case V_IK_OUT: return V{(T)(-k_out) * a.y, (T)k_out * a.x};
+                    case V_IK_COL: return V{(T)(-kc) * a.y, (T)kc * a.x};
+                    case V_LAP: return V{(T)(-k2) * a.x, (T)(-k2) * a.y};
+                    default: return a;
                 }
-            }
-            return acc;
+            };
+            auto gst = [&](int row, int b, V val) {
+                if (b < out_cols && sp.row_out.kept(row)) {
+                    const int r = sp.row_out_compact ? sp.row_out.compact(row) : row;
+                    dst[(long long)r * sp.d_row + b] = val;
+                }
+            };
+            auto smacc = [&](int row, int b) -> V & { return work[row * NB + b]; };
+            fft_columns<T, N, SIGN, NB, NT>(tid, tw, gld, smacc, gst, SyncBlock{});
+            __syncthreads();   // work buffer (and, after the last output, the tile buffer) free again
         }
-    };
-    auto gst = [&](int row, int b, V v) {
-        if (c0 + b < ncols) d[dbase + (long long)row * st.d_row + b] = v;
-    };
-    auto smacc = [&](int row, int b) -> V & { return sm[row * NB + b]; };
-    fft_columns<T, N, SIGN, NB, NT>(tid, tw, gld, smacc, gst, SyncBlock{});
+        buf ^= 1;
+    }
+    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------ z pass
@@ -176,7 +260,7 @@ __device__ __forceinline__ void unpack_r2c(int lane, const V2<T> *line, V2<T> *_
 }
 
 template <typename T, int N, int DIR>
-__global__ void __launch_bounds__(ZWARPS * 32)
+__global__ void __launch_bounds__(ZWARPS * 32, 2)
 k_zpass(FieldSet<T> f, long long nlines, int nz2, T scale, const V2<T> *__restrict__ tw) {
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -219,30 +303,78 @@ k_zpass(FieldSet<T> f, long long nlines, int nz2, T scale, const V2<T> *__restri
 //   4 alpha (lap s c + grad c . grad s) + u . grad c   (colloidAdvectionKernel_mgpu, solver.cu:374-388)
 // One warp per input field; one block per line pair.
 template <typename T, int N> struct ZPCfg {
-    static constexpr int LEN = padded_len<T>(N);
+    static constexpr int LEN = padded_len<T>(N);   // padded line in the work area
+    __host__ __device__ static constexpr int work_bytes(int nph) {
+        return (nph * LEN * (int)sizeof(V2<T>) + 127) / 128 * 128;
+    }
+    // staging area: nraw fields x a line pair of ncp complex values each
+    __host__ __device__ static constexpr int pipe_bytes(int nph, int nraw, int ncp) {
+        return work_bytes(nph) + nraw * 2 * ncp * (int)sizeof(V2<T>) + 16;
+    }
+    static constexpr int SMEM_MAX = 227 * 1024;
 };
 
+// A physical quantity of the z pass is +-raw[r0] (times i kz) +- raw[r1]
+// (times i kz): the kz factors and the two-field combinations of the
+// vorticity are formed here, from the lines already on chip.
+struct ZRecipe { signed char r[2]; signed char ikz[2]; signed char sgn[2]; signed char pad[2]; };
+struct ZRecipeSet { ZRecipe q[MAXF]; };
+
+// C2R packing (see pack_c2r) of a combination of two raw line pairs: a
+// line pair is 2*ncp complex values (line a then line b), of which the first
+// nkz of each line are the kept modes (the rest of the half spectrum is zero).
 template <typename T, int N>
-__global__ void __launch_bounds__(14 * 32)
-k_zphys(FieldSet<T> f, int nin, int nout, long long nlines, int nz2, T scale, T alpha, const V2<T> *__restrict__ tw) {
+__device__ __forceinline__ void pack_c2r_combo(int lane, V2<T> *line, const ZRecipe rc, const V2<T> *a0, const V2<T> *a1,
+                                               int ncp, int nkz, double dkz) {
+    using V = V2<T>;
+    for (int k = lane; k <= N / 2; k += 32) {
+        V a = V{T(0), T(0)}, b = V{T(0), T(0)};
+        if (k < nkz) {
+            const T kz = (T)wavenum(k, N, dkz);
+            a = a0[k];
+            b = a0[ncp + k];
+            if (rc.ikz[0]) { a = V{-kz * a.y, kz * a.x}; b = V{-kz * b.y, kz * b.x}; }
+            if (rc.sgn[0] < 0) { a = V{-a.x, -a.y}; b = V{-b.x, -b.y}; }
+            if (a1) {
+                V c = a1[k], d = a1[ncp + k];
+                if (rc.ikz[1]) { c = V{-kz * c.y, kz * c.x}; d = V{-kz * d.y, kz * d.x}; }
+                if (rc.sgn[1] < 0) { a = csub(a, c); b = csub(b, d); }
+                else { a = cadd(a, c); b = cadd(b, d); }
+            }
+            if (k == 0 || 2 * k == N) { a.y = T(0); b.y = T(0); }
+        }
+        line[padded<T>(k)] = V{a.x - b.y, a.y + b.x};
+        if (k > 0 && 2 * k < N) line[padded<T>(N - k)] = V{a.x + b.y, b.x - a.y};
+    }
+}
+
+// R2C unpacking into a line pair of stride ncp: modes k <= N/2 are written,
+// columns beyond N/2 (padding of short lines) are set to zero.
+template <typename T, int N>
+__device__ __forceinline__ void unpack_r2c_pad(int lane, const V2<T> *line, V2<T> *A, V2<T> *B, int ncp) {
+    using V = V2<T>;
+    for (int k = lane; k < ncp; k += 32) {
+        if (k <= N / 2) {
+            V zk = line[padded<T>(k)];
+            V zm = line[padded<T>((N - k) % N)];
+            A[k] = V{T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
+            B[k] = V{T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
+        } else {
+            A[k] = V{T(0), T(0)};
+            B[k] = V{T(0), T(0)};
+        }
+    }
+}
+
+// Pointwise products of one line pair held in the work area (real part =
+// line a, imaginary part = line b); results overwrite regions 0..4.
+// Regions: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3, 6 sx, 7 sy, 8 sz,
+// [9 cx, 10 cy, 11 cz], [12 c, 13 lap s].
+template <typename T, int N, int NPH>
+__device__ __forceinline__ void zphys_products(V2<T> *reg, T scale, T alpha) {
     using V = V2<T>;
     constexpr int LEN = ZPCfg<T, N>::LEN;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *reg = reinterpret_cast<V *>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long la = 2 * (long long)blockIdx.x, lb = la + 1;
-    const bool hasB = lb < nlines;
-    // phase 1: every warp brings one quantity to physical space
-    if (warp < nin) {
-        V *line = reg + warp * LEN;
-        const V *src = f.p[warp];
-        pack_c2r<T, N>(lane, line, src + la * nz2, src + lb * nz2, hasB);
-        __syncwarp();
-        warp_line_fft<T, N, +1>(lane, line, tw);
-    }
-    __syncthreads();
-    // phase 2: pointwise products on both lines (real part = line a, imag = line b)
-    const bool has_c = nin >= 12, has_al = nin >= 14;
+    constexpr bool has_c = NPH >= 12, has_al = NPH >= 14;
     for (int n = threadIdx.x; n < N; n += blockDim.x) {
         const int pn = padded<T>(n);
         V u = reg[0 * LEN + pn], v = reg[1 * LEN + pn], w = reg[2 * LEN + pn];
@@ -251,16 +383,18 @@ k_zphys(FieldSet<T> f, int nin, int nout, long long nlines, int nz2, T scale, T 
         u = cscale(u, scale); v = cscale(v, scale); w = cscale(w, scale);
         o1 = cscale(o1, scale); o2 = cscale(o2, scale); o3 = cscale(o3, scale);
         sx = cscale(sx, scale); sy = cscale(sy, scale); sz = cscale(sz, scale);
+        // omega x u (crossProductKernel_mgpu, solver.cu:139-164), u . grad s (dotKernel_mgpu, :342-356)
         V n1 = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
         V n2 = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
         V n3 = V{o1.x * v.x - o2.x * u.x, o1.y * v.y - o2.y * u.y};
         V ns = V{u.x * sx.x + v.x * sy.x + w.x * sz.x, u.y * sx.y + v.y * sy.y + w.y * sz.y};
         V nc = V{T(0), T(0)};
-        if (has_c) {
+        if constexpr (has_c) {
+            // colloidAdvectionKernel_mgpu (solver.cu:374-388)
             V cx = cscale(reg[9 * LEN + pn], scale), cy = cscale(reg[10 * LEN + pn], scale);
             V cz = cscale(reg[11 * LEN + pn], scale);
             V adv = V{u.x * cx.x + v.x * cy.x + w.x * cz.x, u.y * cx.y + v.y * cy.y + w.y * cz.y};
-            if (has_al) {
+            if constexpr (has_al) {
                 V cc = cscale(reg[12 * LEN + pn], scale), ls = cscale(reg[13 * LEN + pn], scale);
                 V dr = V{ls.x * cc.x + cx.x * sx.x + cy.x * sy.x + cz.x * sz.x,
                          ls.y * cc.y + cx.y * sx.y + cy.y * sy.y + cz.y * sz.y};
@@ -273,15 +407,86 @@ k_zphys(FieldSet<T> f, int nin, int nout, long long nlines, int nz2, T scale, T 
         reg[1 * LEN + pn] = n2;
         reg[2 * LEN + pn] = n3;
         reg[3 * LEN + pn] = ns;
-        if (has_c) reg[4 * LEN + pn] = nc;
+        if constexpr (has_c) reg[4 * LEN + pn] = nc;
     }
-    __syncthreads();
-    // phase 3: z R2C of the products, written over the input lines
-    if (warp < nout) {
-        V *line = reg + warp * LEN;
-        warp_line_fft<T, N, -1>(lane, line, tw);
-        V *dstp = f.p[warp];
-        unpack_r2c<T, N>(lane, line, dstp + la * nz2, dstp + lb * nz2, hasB);
+}
+
+// Persistent: block b handles line pairs b, b + gridDim.x, ...  Lines are
+// [x][y] rows of ncp complex values (the kept kz modes, zero-padded).  With
+// `pipe` the raw lines (NRAW fields) of the next pair are fetched with
+// cp.async.bulk into a staging area while the current pair is transformed,
+// multiplied and written back; otherwise they are read from global memory
+// directly.  Warp q forms physical quantity q; the products are z-transformed
+// back and written over raw fields 0..nout-1 of the same pair.  A wait that
+// times out sets bit 0 of *err and the block stops.
+template <typename T, int N, int NPH, int NRAW>
+__global__ void __launch_bounds__(NPH * 32, 1)
+k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
+        int ncp, int nkz, int pipe, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw,
+        unsigned *__restrict__ err) {
+    using V = V2<T>;
+    using C = ZPCfg<T, N>;
+    constexpr int LEN = C::LEN;
+    const int rawf = 2 * ncp;
+    const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *reg = reinterpret_cast<V *>(smem_raw);
+    V *raw = reinterpret_cast<V *>(smem_raw + C::work_bytes(NPH));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + C::work_bytes(NPH) + NRAW * raw_bytes);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    long long pair = blockIdx.x;
+    if (pair >= npairs) return;   // uniform for the block
+    if (pipe) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    auto issue = [&](long long p) {
+        mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
+        for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+    };
+    if (pipe && threadIdx.x == 0) issue(pair);
+    unsigned parity = 0;
+    V *line = reg + warp * LEN;
+    const ZRecipe rc = zr.q[warp];
+    for (; pair < npairs; pair += gridDim.x) {
+        const V *a0, *a1;
+        if (pipe) {
+            const bool ok = mbar_wait_bounded(bar, parity);
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicOr(err, 1u);
+                mbar_wait_bounded(bar, parity);   // let an overdue copy land before leaving
+                return;
+            }
+            parity ^= 1u;
+            a0 = raw + rc.r[0] * rawf;
+            a1 = rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr;
+        } else {
+            a0 = f.p[rc.r[0]] + pair * rawf;
+            a1 = rc.r[1] >= 0 ? f.p[rc.r[1]] + pair * rawf : nullptr;
+        }
+        pack_c2r_combo<T, N>(lane, line, rc, a0, a1, ncp, nkz, dkz);
+        __syncthreads();   // staging area (or the raw lines in global memory) consumed
+        if (pipe) {
+            const long long next = pair + gridDim.x;
+            if (threadIdx.x == 0 && next < npairs) {
+                fence_proxy_async_smem();
+                issue(next);
+            }
+        }
+        __syncwarp();
+        warp_line_fft<T, N, +1>(lane, line, tw);   // every quantity to physical space
+        __syncthreads();
+        zphys_products<T, N, NPH>(reg, scale, alpha);
+        __syncthreads();
+        if (warp < nout) {   // z R2C of the products, written over raw fields 0..nout-1
+            warp_line_fft<T, N, -1>(lane, line, tw);
+            V *d = f.p[warp] + pair * rawf;
+            unpack_r2c_pad<T, N>(lane, line, d, d + ncp, ncp);
+        }
+        __syncthreads();   // work area reused by the next pair
     }
 }
 
@@ -291,61 +496,86 @@ struct UpdCoef {
     int scheme;       // GNSS_SCHEME_*
     int euler;        // CN/AB2: first step
     double dt;
-    double num[5];    // CN: reference "num" (Re, Re*Sc, Re*Sc_c)
+    double hnum[5];   // CN: dt / 2 / num with the reference's num (Re, Re*Sc, Re*Sc_c)
     double nu[5];     // IF: diffusivity per field
     double gam, zet_next, alph;   // IF-RK3 substep coefficients
     int substep;      // IF-RK3: 0, 1, 2 (substep 0 ignores the history input)
 };
 
+// One thread per spectral mode (grid-stride).  The arithmetic follows
+// makeRHS / deAlias / timestep / update (solver.cu:461-657) with the divisions
+// by k^2 and by (1 + dt k^2/(2 num)) done once as reciprocals.
+// Modes are enumerated in the kept box (kept ky, kept kx, kz < nkz); nl is
+// the compact [kyc][kxc][ncp] layout of the forward passes; state and hist
+// use the reference layout.  Modes outside the box are neither read nor
+// written: they stay zero once the state has been dealiased.
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_update(FieldSet<T> state, FieldSet<T> hist, FieldSet<T> nl, Geom g, UpdCoef c) {
+k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
+         const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
+         UpdCoef c) {
     using V = V2<T>;
-    const long long nspec = (long long)g.nx * g.ny * g.nz2;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < nspec;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const int kzi = (int)(idx % g.nz2);
-        const long long t = idx / g.nz2;
-        const int kxi = (int)(t % g.nx);
-        const int kyi = (int)(t / g.nx);
+    const int nkx = kx_keep.count(), nky = ky_keep.count();
+    const long long nmodes = (long long)nky * nkx * nkz;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nmodes;
+         m += (long long)gridDim.x * blockDim.x) {
+        const int kzi = (int)(m % nkz);
+        const long long t = m / nkz;
+        const int kxc = (int)(t % nkx);
+        const int kyc = (int)(t / nkx);
+        const int kxi = kx_keep.expand(kxc), kyi = ky_keep.expand(kyc);
+        const long long idx = ((long long)kyi * g.nx + kxi) * g.nz2 + kzi;      // state / hist
+        const long long jdx = ((long long)kyc * nkx + kxc) * ncp + kzi;         // nonlinear term
         const double k1 = wavenum(kxi, g.nx, g.dkx), k2 = wavenum(kyi, g.ny, g.dky), k3 = wavenum(kzi, g.nz, g.dkz);
         const double ksq = ksq3(k1, k2, k3);
         const bool masked = ksq > g.kmax2;
+        const bool zero_mode = (kxi == 0 && kyi == 0 && kzi == 0);
         double R[5][2];
-        // makeRHS (solver.cu:461-521): (k k^T / k^2 - I) N for the velocity,
-        // -N for the scalars, zero at k = 0; then deAlias(rhs) (solver.cu:756)
-        if ((kxi == 0 && kyi == 0 && kzi == 0) || masked) {
+        // makeRHS: (k k^T / k^2 - I) N for the velocity, -N for the scalars,
+        // zero at k = 0; then deAlias(rhs) (solver.cu:756)
+        if (zero_mode || masked) {
+#pragma unroll
             for (int q = 0; q < 5; ++q) R[q][0] = R[q][1] = 0.0;
         } else {
-            V a = nl.p[0][idx], b = nl.p[1][idx], cc = nl.p[2][idx];
-            double t1r = a.x, t1c = a.y, t2r = b.x, t2c = b.y, t3r = cc.x, t3c = cc.y;
-            R[0][0] = (k1 * k1 / ksq - 1.0) * t1r + (k1 * k2 / ksq) * t2r + (k1 * k3 / ksq) * t3r;
-            R[0][1] = (k1 * k1 / ksq - 1.0) * t1c + (k1 * k2 / ksq) * t2c + (k1 * k3 / ksq) * t3c;
-            R[1][0] = (k2 * k1 / ksq) * t1r + (k2 * k2 / ksq - 1.0) * t2r + (k2 * k3 / ksq) * t3r;
-            R[1][1] = (k2 * k1 / ksq) * t1c + (k2 * k2 / ksq - 1.0) * t2c + (k2 * k3 / ksq) * t3c;
-            R[2][0] = (k3 * k1 / ksq) * t1r + (k3 * k2 / ksq) * t2r + (k3 * k3 / ksq - 1.0) * t3r;
-            R[2][1] = (k3 * k1 / ksq) * t1c + (k3 * k2 / ksq) * t2c + (k3 * k3 / ksq - 1.0) * t3c;
-            for (int q = 3; q < c.nf; ++q) {
-                V s = nl.p[q][idx];
-                R[q][0] = -(double)s.x;
-                R[q][1] = -(double)s.y;
+            const double ik = 1.0 / ksq;
+            const V a = nl.p[0][jdx], b = nl.p[1][jdx], cc = nl.p[2][jdx];
+            const double pr = (k1 * (double)a.x + k2 * (double)b.x + k3 * (double)cc.x) * ik;   // k . N / k^2
+            const double pi = (k1 * (double)a.y + k2 * (double)b.y + k3 * (double)cc.y) * ik;
+            R[0][0] = k1 * pr - (double)a.x;
+            R[0][1] = k1 * pi - (double)a.y;
+            R[1][0] = k2 * pr - (double)b.x;
+            R[1][1] = k2 * pi - (double)b.y;
+            R[2][0] = k3 * pr - (double)cc.x;
+            R[2][1] = k3 * pi - (double)cc.y;
+#pragma unroll
+            for (int q = 3; q < 5; ++q) {
+                if (q < c.nf) {
+                    const V s = nl.p[q][jdx];
+                    R[q][0] = -(double)s.x;
+                    R[q][1] = -(double)s.y;
+                } else {
+                    R[q][0] = R[q][1] = 0.0;
+                }
             }
         }
-        for (int q = 0; q < c.nf; ++q) {
-            V fv = state.p[q][idx];
-            double fr = masked ? 0.0 : (double)fv.x, fi = masked ? 0.0 : (double)fv.y;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            if (q >= c.nf) break;
+            const V fv = state.p[q][idx];
+            const double fr = masked ? 0.0 : (double)fv.x, fi = masked ? 0.0 : (double)fv.y;
             if (c.scheme == 0) {
                 // eulerKernel_mgpu / adamsBashforthKernel_mgpu (solver.cu:547-585)
-                const double a = 1.0 - c.dt / 2.0 * ksq / c.num[q];
-                const double bb = 1.0 + c.dt / 2.0 * ksq / c.num[q];
+                const double hk = c.hnum[q] * ksq;
+                const double a = 1.0 - hk;
+                const double ib = 1.0 / (1.0 + hk);
                 double nr, ni;
                 if (c.euler) {
-                    nr = (a * fr + c.dt * R[q][0]) / bb;
-                    ni = (a * fi + c.dt * R[q][1]) / bb;
+                    nr = (a * fr + c.dt * R[q][0]) * ib;
+                    ni = (a * fi + c.dt * R[q][1]) * ib;
                 } else {
-                    V ro = hist.p[q][idx];
-                    nr = (a * fr + c.dt * (1.5 * R[q][0] - 0.5 * (double)ro.x)) / bb;
-                    ni = (a * fi + c.dt * (1.5 * R[q][1] - 0.5 * (double)ro.y)) / bb;
+                    const V ro = hist.p[q][idx];
+                    nr = (a * fr + c.dt * (1.5 * R[q][0] - 0.5 * (double)ro.x)) * ib;
+                    ni = (a * fi + c.dt * (1.5 * R[q][1] - 0.5 * (double)ro.y)) * ib;
                 }
                 state.p[q][idx] = V{(T)nr, (T)ni};
                 hist.p[q][idx] = V{(T)R[q][0], (T)R[q][1]};   // updateKernel_mgpu (solver.cu:618-637)
@@ -353,7 +583,7 @@ k_update(FieldSet<T> state, FieldSet<T> hist, FieldSet<T> nl, Geom g, UpdCoef c)
                 const double E = exp(-c.nu[q] * ksq * c.alph * c.dt);
                 double hr = 0.0, hi = 0.0;
                 if (c.substep > 0) {
-                    V h = hist.p[q][idx];
+                    const V h = hist.p[q][idx];
                     hr = (double)h.x;
                     hi = (double)h.y;
                 }

@@ -85,6 +85,7 @@ _SIGS = {
     "gnss_stats": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_run_host": [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_launch_count": [_VP],
+    "gnss_check": [_VP, _VP],
     "gnss_profile_enable": [_VP, ctypes.c_int],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
 }
@@ -305,6 +306,10 @@ class Context:
                 else ctypes.cast(stats.data_ptr(), ctypes.POINTER(ctypes.c_double))
         self._ck(self.lib.gnss_run_host(self._h, _host_ptr(host_in), _host_ptr(host_out), int(n_steps),
                                         int(bool(first_euler)), sp, _stream(stream)), "gnss_run_host")
+
+    def check(self, stream=None) -> None:
+        """Synchronise and raise if a bounded device wait timed out."""
+        self._ck(self.lib.gnss_check(self._h, _stream(stream)), "gnss_check")
 
     # -- instrumentation ------------------------------------------------------
     def launch_count(self) -> int:

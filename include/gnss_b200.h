@@ -12,6 +12,8 @@
  * with nz2 = nz/2 + 1; a field buffer holds nx*ny*nz2 complex values and is
  * used in place for both views, exactly like the reference.  Element type is
  * double (GNSS_FP64) or float (GNSS_FP32) per the context's precision.
+ * Device pointers must be aligned to one complex element (16 bytes for FP64,
+ * 8 for FP32); misaligned pointers are rejected with GNSS_ERR_INVALID.
  *
  * Differences from the reference, all deliberate:
  *   - sizes and parameters are runtime values (gnss_config) instead of the
@@ -40,6 +42,7 @@ typedef int gnss_status;
 #define GNSS_ERR_CUDA 2          /* a CUDA runtime call or kernel launch failed       */
 #define GNSS_ERR_NOMEM 3         /* device or pinned allocation failed                */
 #define GNSS_ERR_UNSUPPORTED 4   /* operation not available for this configuration    */
+#define GNSS_ERR_TIMEOUT 5       /* a bounded device-side wait gave up (see gnss_check) */
 
 #define GNSS_SCHEME_CNAB2 0      /* reference scheme: Euler/CN first step, AB2/CN after (solver.cu:547-616) */
 #define GNSS_SCHEME_RK3IF 1      /* low-storage RK3 (Wray) with integrating factor exp(-nu k^2 dt)          */
@@ -130,6 +133,12 @@ gnss_status gnss_colloid_advection(gnss_ctx *ctx, const void *u, const void *v, 
                                    void *stream);                                    /* colloidAdvection, solver.cu:374-405 */
 
 /* One full time step of the fused B200 path (solver_ps, solver.cu:700-765).
+ * The transforms are pruned to the dealiasing truncation: state modes whose
+ * wavenumber along any axis exceeds the truncation radius are neither read
+ * nor written, so they must be zero on entry (gnss_dealias does that, as the
+ * reference does once before its loop, main.cu:156, and at the start of
+ * every step, solver.cu:704); within the kept box the step applies the
+ * spherical mask itself and leaves exact zeros outside the sphere.
  * state: spectral u, v, w, s (and c).  hist: for GNSS_SCHEME_CNAB2 the
  * previous RHS (the reference's rhs_old; read when euler == 0, always
  * written); unused (may be NULL) for GNSS_SCHEME_RK3IF.  euler selects the
@@ -143,13 +152,20 @@ gnss_status gnss_stats(gnss_ctx *ctx, const gnss_fields *state, double *out, voi
 
 /* End-to-end call with host buffers: copies the packed host state
  * (3 + n_scalars spectral fields back to back) to context-owned device
- * buffers, runs n_steps steps (the first one Euler when first_euler != 0 for
+ * buffers, dealiases it (main.cu:156), runs n_steps steps (the first one
+ * Euler when first_euler != 0 for
  * GNSS_SCHEME_CNAB2; hist starts at zero), records the statistics after each
  * step into stats_out (n_steps * GNSS_NSTATS doubles, may be NULL) and copies
  * the final state back into host_state_out (may alias host_state_in).
  * Synchronises the stream before returning. */
 gnss_status gnss_run_host(gnss_ctx *ctx, const void *host_state_in, void *host_state_out, int n_steps,
                           int first_euler, double *stats_out, void *stream);
+
+/* Synchronises the stream and reports GNSS_ERR_TIMEOUT if any kernel of this
+ * context gave up a bounded wait since the last check (the flag is then
+ * cleared).  No counterpart in the reference, which has no device-side waits.
+ * gnss_stats and gnss_run_host perform this check themselves. */
+gnss_status gnss_check(gnss_ctx *ctx, void *stream);
 
 /* Instrumentation (no counterpart in the reference, which only brackets its
  * loop with cudaProfilerStart/Stop, main.cu:171,249).

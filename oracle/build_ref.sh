@@ -3,7 +3,9 @@
 # vector generator and the reference arm of bench.py) from the unmodified
 # sources in the reference checkout, one executable per grid configuration:
 #
-#     oracle/_ref/<cfg>/refdrv
+#     oracle/_ref/<cfg>/refdrv        the reference's solver.o + fftfuncs.o (cuFFT)
+#     oracle/_ref/<cfg>/refdrv_gnss   the same program linked against the B200
+#                                     library through gnss-1_b200/refabi/refabi.cu
 #
 # The reference fixes every size and parameter at compile time in dnsparams.h
 # (dnsparams.h:9-41).  For each configuration this script creates
@@ -19,6 +21,7 @@ HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF="${GNSS_REFERENCE_DIR:-/root/reference}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
+LIB="$HERE/../gnss-1_b200"
 FLAGS=(-O3 -gencode arch=compute_100a,code=sm_100a -Xcompiler -w -w)
 
 if [ ! -f "$REF/solver.cu" ]; then
@@ -97,7 +100,19 @@ build_one() {
     done
     "$NVCC" "${FLAGS[@]}" -dc -I"$HERE/refshim" -I"$d/src" -o "$d/obj/refdriver.o" "$HERE/refdriver.cu"
     "$NVCC" "${FLAGS[@]}" -o "$d/refdrv" "${objs[@]}" "$d/obj/refdriver.o" -lcufft
-    # keep only the executable: the links into the reference tree stay here
+    # drop-in variant: the same driver and the reference's remaining objects, with
+    # solver.o and fftfuncs.o replaced by the B200 library's reference-ABI shim
+    if [ -f "$LIB/libgnss_b200.so" ]; then
+        "$NVCC" "${FLAGS[@]}" -dc -I"$HERE/../include" -I"$d/src" -o "$d/obj/refabi.o" \
+            "$HERE/../gnss-1_b200/refabi/refabi.cu"
+        local keep=()
+        for o in "${objs[@]}"; do
+            case "$(basename "$o")" in solver.o|fftfuncs.o) ;; *) keep+=("$o") ;; esac
+        done
+        "$NVCC" "${FLAGS[@]}" -o "$d/refdrv_gnss" "${keep[@]}" "$d/obj/refabi.o" "$d/obj/refdriver.o" \
+            -L"$LIB" -lgnss_b200 -lcufft -Xlinker -rpath -Xlinker '$ORIGIN/../../../gnss-1_b200'
+    fi
+    # keep only the executables: the links into the reference tree stay here
     rm -rf "$d/src" "$d/obj"
     echo "built $d/refdrv"
 }

@@ -100,3 +100,43 @@ def test_live_reference_256_two_scalars(torch_cuda):
                 worst = max(worst, rel)
                 assert rel < 1e-9, (s, k, stats[k], ref_stats[s][i])
     print(f"worst statistic deviation over {steps} steps: {worst:.2e}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg,n,ns,steps", [("g16a", 16, 2, 4), ("c64", 64, 1, 5)])
+def test_dropin_shim_matches_reference_program(torch_cuda, cfg, n, ns, steps):
+    """The same driver linked two ways: the reference's solver.o + fftfuncs.o
+    (refdrv) and the B200 library through the reference-ABI shim
+    (refdrv_gnss, gnss-1_b200/refabi/refabi.cu).  States and statistics agree."""
+    from golden.make_golden import initial_state
+    ref = _refdrv(cfg)
+    new = ref.parent / "refdrv_gnss"
+    if not new.exists():
+        pytest.skip("drop-in build not present")
+    f = initial_state(n, ns, 21, min(8.0, n / 4))
+    dumps = f"1,{steps}"
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        with open(td / "ic.bin", "wb") as fp:
+            for a in f:
+                fp.write(np.ascontiguousarray(a).tobytes())
+        for name, exe in (("ref", ref), ("new", new)):
+            d = td / name
+            d.mkdir()
+            r = subprocess.run([str(exe), "run", str(td / "ic.bin"), str(steps), str(d), dumps],
+                               capture_output=True, text=True, timeout=600)
+            assert r.returncode == 0, r.stderr[-2000:]
+            out[name] = {
+                "stats": np.fromfile(d / "stats.bin", dtype=np.float64).reshape(steps + 1, 7),
+                "s1": np.fromfile(d / "state_1.bin", dtype=np.complex128).reshape(5, -1),
+                "sN": np.fromfile(d / f"state_{steps}.bin", dtype=np.complex128).reshape(5, -1),
+                "hN": np.fromfile(d / f"rhsold_{steps}.bin", dtype=np.complex128).reshape(5, -1),
+            }
+    for q in range(3 + ns):
+        assert rel_l2(out["new"]["s1"][q], out["ref"]["s1"][q]) < 1e-12
+        assert rel_l2(out["new"]["sN"][q], out["ref"]["sN"][q]) < 1e-11
+        assert rel_l2(out["new"]["hN"][q], out["ref"]["hN"][q]) < 1e-11
+    a, b = out["new"]["stats"], out["ref"]["stats"]
+    mask = b != 0
+    assert np.all(np.abs(a[mask] - b[mask]) <= 1e-10 * np.abs(b[mask]))

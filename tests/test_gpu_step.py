@@ -75,6 +75,7 @@ def test_step_rk3if_fp64(torch_cuda, oracle, ns):
     f = [a.copy() for a in init]
     with G.Context(n, re=re, sc=0.7, sc_c=1.3, dt=dt, n_scalars=ns, scheme=G.GNSS_SCHEME_RK3IF) as ctx:
         st = [to_dev(torch, a) for a in init]
+        ctx.de_alias(st)
         for s in range(4):
             oracle.step_rk3if(oc, f, ns)
             ctx.solver_ps(st, None, euler=False)
@@ -143,6 +144,7 @@ def test_run_host_matches_device_steps(torch_cuda):
     with G.Context(n, n_scalars=ns, re=800.0, dt=1e-3) as ctx:
         st = [to_dev(torch, a) for a in init]
         hi = [torch.zeros_like(st[0]) for _ in st]
+        ctx.de_alias(st)     # gnss_run_host dealiases the uploaded state the same way
         for s in range(steps):
             ctx.solver_ps(st, hi, euler=(s == 0))
         last = ctx.stats(st)
