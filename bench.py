@@ -103,6 +103,24 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(x: float) -> float:
+    """Max of a per-rank scalar over the process group (identity without one).
+    Times are the slowest rank's: every rank advances its own jet (replicas)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = f"cuda:{torch.cuda.current_device()}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(points: float, ms_max: float, world: int) -> float:
+    """Whole-job Mpoint-steps/s: every rank advanced `points` per step in ms_max."""
+    return world * points / (ms_max * 1e-3) / 1e6
+
+
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -236,30 +254,26 @@ def ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device(f"cuda:{dev}"))
         barrier = dist.barrier
-
-        def red(x, op="max"):
-            t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
-            return float(t.item())
+        red = max_over_ranks
     prec = G.GNSS_FP32 if args.precision == "mixed" else G.GNSS_FP64
     scheme = G.GNSS_SCHEME_CNAB2 if args.scheme == "cnab2" else G.GNSS_SCHEME_RK3IF
     n = args.n
     leg = run_leg(G, torch, n, prec, scheme, args.steps, args.warmup, dev, barrier=barrier)
     ms = leg["ms"] if red is None else red(leg["ms"])
     pts = float(n) ** 3
-    value = ws * pts / (ms * 1e-3) / 1e6
+    value = replica_value(pts, ms, ws)
     fp64 = None
     if prec == G.GNSS_FP32 and not args.no_fp64_leg:
         l64 = run_leg(G, torch, n, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier)
         ms64 = l64["ms"] if red is None else red(l64["ms"])
-        fp64 = {"value": round(ws * pts / (ms64 * 1e-3) / 1e6, 3), "ms_per_step": round(ms64, 4),
+        fp64 = {"value": round(replica_value(pts, ms64, ws), 3), "ms_per_step": round(ms64, 4),
                 "mixed_over_fp64": round(ms64 / ms, 3),
                 "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in l64["profile"].items()}}
     e2e = None
     if not args.no_e2e:
         e = run_e2e(G, torch, n, prec, scheme, args.e2e_calls, dev)
         ms_call = e["ms_call"] if red is None else red(e["ms_call"])
-        e2e = {"value": round(ws * pts * E2E_STEPS_PER_CALL / (ms_call * 1e-3) / 1e6, 3), "unit": UNIT,
+        e2e = {"value": round(replica_value(pts * E2E_STEPS_PER_CALL, ms_call, ws), 3), "unit": UNIT,
                "h2d_bytes_per_step": int(e["h2d"]), "d2h_bytes_per_step": int(e["d2h"]),
                "steps_per_call": E2E_STEPS_PER_CALL,
                "call": "gnss_run_host: pinned host state in, steps, per-step statistics and state out"}
