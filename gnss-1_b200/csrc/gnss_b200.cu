@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1119,3 +1120,100 @@ gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int 
     return gnss_check(c, stream);
 }
 
+
+// ============================================================== allocation-free forward transform
+// For callers that may not allocate device memory at all: code running under
+// a memory manager that owns every byte of the device (a framework's caching
+// allocator, a fixed per-process budget) and latency-critical loops in which
+// a cudaMalloc / cudaFree would synchronise the device.  gnss_forward_noalloc
+// computes exactly what gnss_forward computes, but its twiddle tables and its
+// one-field scratch live in the file-scope array below instead of in a
+// context, and it never calls cudaMalloc, cudaFree or any allocating routine.
+//
+// Layout of the array: three twiddle tables of GNSS_NOALLOC_TW complex values
+// (x, y, z), then GNSS_NOALLOC_MAX_ELEMS complex values of scratch.  Sizes are
+// in double2 units, so the same storage serves FP32 (float2) with room to
+// spare.  Every GPU that loads the library holds the array until the process
+// exits.  All calls share it: it keeps the last call's contents (each call
+// rewrites the twiddles it uses and overwrites the scratch it reads), and
+// calls that overlap on the GPU, on any stream, race on it.
+constexpr size_t GNSS_NOALLOC_TW = 512;
+static __device__ __align__(256) double2 g_noalloc_pool[3 * GNSS_NOALLOC_TW + GNSS_NOALLOC_MAX_ELEMS];
+
+// Host-side address of the array on each device, looked up once per device
+// (the symbol itself is only a host stand-in, not a device address).
+static void *g_noalloc_addr[64];
+static bool g_noalloc_ready[64];
+static std::mutex g_noalloc_mu;
+
+static gnss_status noalloc_pool_address(int dev, void **out) {
+    if (dev < 0 || dev >= 64) return GNSS_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ready[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_pool) != cudaSuccess) {
+            cudaGetLastError();
+            return GNSS_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = p;
+        g_noalloc_ready[dev] = true;
+    }
+    *out = g_noalloc_addr[dev];
+    return GNSS_OK;
+}
+
+template <typename T> static cudaError_t noalloc_twiddles(V2<T> *dst, int n, cudaStream_t s) {
+    V2<T> h[GNSS_NOALLOC_TW];
+    const long double twopi = 6.283185307179586476925286766559L;
+    for (int k = 0; k < n; ++k) {
+        long double a = twopi * (long double)k / (long double)n;
+        h[k].x = (T)cosl(a);
+        h[k].y = (T)(-sinl(a));
+    }
+    // pageable source: the call returns once the table has been staged
+    return cudaMemcpyAsync(dst, h, sizeof(V2<T>) * n, cudaMemcpyHostToDevice, s);
+}
+
+template <typename T> static gnss_status noalloc_forward_t(gnss_ctx *c, void *field, cudaStream_t s) {
+    V2<T> *tw = reinterpret_cast<V2<T> *>(c->tw[0]);
+    const int ns[3] = {c->cfg.nx, c->cfg.ny, c->cfg.nz};
+    for (int a = 0; a < 3; ++a) {
+        c->tw[a] = tw + (size_t)a * GNSS_NOALLOC_TW;
+        CK(c, noalloc_twiddles<T>(reinterpret_cast<V2<T> *>(c->tw[a]), ns[a], s));
+    }
+    return forward_t<T>(c, field, s);
+}
+
+gnss_status gnss_forward_noalloc(const gnss_config *cfg, void *field, void *stream) {
+    if (!cfg || !field) return GNSS_ERR_INVALID;
+    const gnss_config &k = *cfg;
+    if (!size_ok(k.nx) || !size_ok(k.ny) || !size_ok(k.nz)) return GNSS_ERR_INVALID;
+    if (k.precision != GNSS_FP64 && k.precision != GNSS_FP32) return GNSS_ERR_INVALID;
+    if (!(k.lx > 0 && k.ly > 0 && k.lz > 0)) return GNSS_ERR_INVALID;
+    const size_t nspec = (size_t)k.nx * k.ny * (k.nz / 2 + 1);
+    if (nspec > GNSS_NOALLOC_MAX_ELEMS) return GNSS_ERR_INVALID;   // beyond the static scratch
+    const size_t elem = k.precision == GNSS_FP64 ? sizeof(double2) : sizeof(float2);
+    if (reinterpret_cast<uintptr_t>(field) % elem) return GNSS_ERR_INVALID;
+    if (cudaSetDevice(k.device) != cudaSuccess) {
+        cudaGetLastError();
+        return GNSS_ERR_CUDA;
+    }
+    void *pool = nullptr;
+    gnss_status st = noalloc_pool_address(k.device, &pool);
+    if (st) return st;
+    // a context on the stack that points into the static array: no device
+    // allocation happens below (ensure_scratch finds its one field present)
+    gnss_ctx c;
+    c.cfg = k;
+    c.g.nx = k.nx; c.g.ny = k.ny; c.g.nz = k.nz; c.g.nz2 = k.nz / 2 + 1;
+    c.g.dkx = 2 * M_PI / k.lx;
+    c.g.dky = 2 * M_PI / k.ly;
+    c.g.dkz = 2 * M_PI / k.lz;
+    c.nspec = nspec;
+    c.elem = elem;
+    c.tw[0] = pool;
+    c.scratch = reinterpret_cast<double2 *>(pool) + 3 * GNSS_NOALLOC_TW;
+    c.nscratch = 1;
+    cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, k.device);
+    return PREC_CALL(&c, noalloc_forward_t, &c, field, S(stream));
+}

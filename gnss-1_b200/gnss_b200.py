@@ -86,6 +86,7 @@ _SIGS = {
     "gnss_run_host": [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_launch_count": [_VP],
     "gnss_check": [_VP, _VP],
+    "gnss_forward_noalloc": [ctypes.POINTER(GnssConfig), _VP, _VP],
     "gnss_profile_enable": [_VP, ctypes.c_int],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
 }

@@ -181,6 +181,24 @@ long long gnss_launch_count(const gnss_ctx *ctx);
 gnss_status gnss_profile_enable(gnss_ctx *ctx, int on);
 gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 
+/* Forward transform that allocates nothing.  No counterpart in the
+ * reference.  For callers that may not allocate device memory: code running
+ * under a memory manager that owns the whole device (a framework's caching
+ * allocator, a fixed budget) and latency-critical loops where cudaMalloc or
+ * cudaFree would synchronise the device.  Same result as gnss_forward on the
+ * same configuration, but without a context: twiddles and the one-field
+ * scratch live in a static device array of the library (about 18 MB, held on
+ * every GPU that loads the library until the process exits), so the field
+ * must satisfy nx*ny*(nz/2+1) <= GNSS_NOALLOC_MAX_ELEMS (128^3 fits);
+ * larger sizes, like other bad arguments, return GNSS_ERR_INVALID.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the array and keep the last
+ * call's contents in it; calls that overlap on the GPU (any stream, any
+ * thread) race and must be serialised by the caller.  Only cfg's sizes, box
+ * lengths, precision and device are used. */
+#define GNSS_NOALLOC_MAX_ELEMS 1114112
+gnss_status gnss_forward_noalloc(const gnss_config *cfg, void *field, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
