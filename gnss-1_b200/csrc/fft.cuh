@@ -140,6 +140,13 @@ template <int S, typename V> struct Dft<8, S, V> {
 struct SyncBlock { __device__ __forceinline__ void operator()() const { __syncthreads(); } };
 struct SyncWarp { __device__ __forceinline__ void operator()() const { __syncwarp(); } };
 struct SyncNone { __device__ __forceinline__ void operator()() const {} };
+// named barrier shared by a subset of the block's warps (ids 1..15; 0 is __syncthreads)
+struct SyncNamed {
+    int id, nthreads;
+    __device__ __forceinline__ void operator()() const {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+    }
+};
 
 template <typename T, int N, int STAGE, int SIGN, int NB, int NT, bool MIDSYNC, class LD, class ST, class SYNC>
 __device__ __forceinline__ void fft_stage(int tid, const V2<T> *__restrict__ tw, LD ld, ST st, SYNC sync) {
@@ -179,6 +186,41 @@ __device__ __forceinline__ void fft_stage(int tid, const V2<T> *__restrict__ tw,
             const int idxD = (jj / NS) * NS * R + k;
 #pragma unroll
             for (int r = 0; r < R; ++r) st(idxD + r * NS, b, v[p][r]);
+        }
+    }
+}
+
+// A stage whose source and destination buffers differ: each butterfly is
+// stored as soon as it is computed, so a thread holds one butterfly at a time.
+template <typename T, int N, int STAGE, int SIGN, int NB, int NT, class LD, class ST>
+__device__ __forceinline__ void fft_stage_stream(int tid, const V2<T> *__restrict__ tw, LD ld, ST st) {
+    using V = V2<T>;
+    constexpr int R = plan_radix(N, STAGE);
+    constexpr int NS = plan_span(N, STAGE);
+    constexpr int M = N / R;
+    constexpr int NJ = M * NB;
+    constexpr int PER = (NJ + NT - 1) / NT;
+    constexpr int TSTEP = N / (NS * R);
+#pragma unroll 1
+    for (int p = 0; p < PER; ++p) {
+        const int job = tid + p * NT;
+        if ((NJ % NT == 0) || job < NJ) {
+            const int b = job % NB, jj = job / NB;
+            V v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = ld(jj + r * M, b);
+            if (NS > 1) {
+                const int k = jj % NS;
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    V w = __ldg(&tw[r * k * TSTEP]);
+                    v[r] = (SIGN < 0) ? cmul(v[r], w) : cmulc(v[r], w);
+                }
+            }
+            Dft<R, SIGN, V>::run(v);
+            const int idxD = (jj / NS) * NS * R + jj % NS;
+#pragma unroll
+            for (int r = 0; r < R; ++r) st(idxD + r * NS, b, v[r]);
         }
     }
 }
@@ -285,8 +327,8 @@ __device__ __forceinline__ void fft_rest_stages(int tid, const V2<T> *tw, SM sm,
 }
 
 // Padded index for one contiguous line in shared memory: one spare element
-// every 8 (double2) or 16 (float2) entries keeps the stride-R stores of the
-// early stages free of bank conflicts.
+// every 8 (double2) or 16 (float2) entries spreads the stride-8 stores of
+// the radix-8 stages over the banks (measured best of the two spacings).
 template <typename T> __host__ __device__ constexpr int pad_div() { return sizeof(T) == 8 ? 8 : 16; }
 template <typename T> __host__ __device__ __forceinline__ constexpr int padded(int i) { return i + i / pad_div<T>(); }
 template <typename T> __host__ __device__ constexpr int padded_len(int n) { return n + n / pad_div<T>() + 1; }

@@ -184,15 +184,15 @@ template <typename T, int N> struct Launch {
         kern<<<grid, ZWARPS * 32, C::SMEM, s>>>(f, nlines, nz2, scale, t);
         return cudaGetLastError();
     }
-    template <int NPH, int NRAW>
-    static cudaError_t zphys_n(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
+    template <int NPH, int NRAW, bool PP>
+    static cudaError_t zphys_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
                                int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
                                cudaStream_t s) {
         using C = ZPCfg<T, N>;
-        const int pipe_b = C::pipe_bytes(NPH, NRAW, ncp);
+        const int pipe_b = C::pipe_bytes(NPH, NRAW, ncp, PP);
         const int pipe = pipe_b <= C::SMEM_MAX ? 1 : 0;
-        const int smem = pipe ? pipe_b : C::work_bytes(NPH);
-        auto kern = k_zphys<T, N, NPH, NRAW>;
+        const int smem = pipe ? pipe_b : C::work_bytes(NPH, PP);
+        auto kern = k_zphys<T, N, NPH, NRAW, PP>;
         cudaError_t e = prep_smem(kern, smem);
         if (e != cudaSuccess) return e;
         int per_sm = blocks_per_sm(kern, NPH * 32, smem);
@@ -202,6 +202,16 @@ template <typename T, int N> struct Launch {
         kern<<<(unsigned)grid, NPH * 32, smem, s>>>(f, zr, nout, npairs, ncp, nkz, pipe, scale, alpha, dkz,
                                                      reinterpret_cast<const V2<T> *>(tw), err);
         return cudaGetLastError();
+    }
+    // ping-pong banks when they fit next to the staging area, else in place
+    template <int NPH, int NRAW>
+    static cudaError_t zphys_n(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
+                               int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
+                               cudaStream_t s) {
+        using C = ZPCfg<T, N>;
+        if (C::pipe_bytes(NPH, NRAW, ncp, true) <= C::SMEM_MAX)
+            return zphys_k<NPH, NRAW, true>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+        return zphys_k<NPH, NRAW, false>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
     }
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,

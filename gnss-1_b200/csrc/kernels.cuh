@@ -102,26 +102,33 @@ template <typename T, int N> struct PassCfg {
     static constexpr int ELEM = (int)sizeof(V2<T>);
     static constexpr int NB0 = (64 * 1024 / ELEM) / N;
     static constexpr int NB = pow2_floor(NB0 > 16 ? 16 : (NB0 < 1 ? 1 : NB0));
-    static constexpr int E = (sizeof(T) == 8) ? 8 : 16;
-    static constexpr int NT0 = N * NB / E;
-    static constexpr int NT = NT0 < 32 ? 32 : (NT0 > 1024 ? 1024 : NT0);
+    static constexpr int NT0 = N * NB / 8;   // one radix-8 butterfly per thread, at most 512 threads
+    static constexpr int NT = NT0 < 32 ? 32 : (NT0 > 512 ? 512 : NT0);
+    static constexpr int E = N * NB / NT;
     static constexpr int TILE = N * NB;
     static constexpr bool WORK = plan_nstages(N) > 1;
     static constexpr int SMEM = (2 + (WORK ? 1 : 0)) * TILE * ELEM;
 };
 
 // Asynchronous copy of one tile (rows kept by row_in, columns < ncols; the
-// rest zero-filled) into shared memory, laid out [row][NB].
-template <typename T>
-__device__ __forceinline__ void tile_prefetch(V2<T> *dst, const V2<T> *__restrict__ src, const PassSpec &sp, int tile,
-                                              int nb, int c0, int tid, int nt) {
-    for (int e = tid; e < tile; e += nt) {
-        const int row = e / nb, b = e % nb;
-        const bool ok = (c0 + b < sp.ncols) && sp.row_in.kept(row);
-        const int r = ok ? (sp.row_in_compact ? sp.row_in.compact(row) : row) : 0;
-        const V2<T> *p = src + (ok ? (long long)r * sp.s_row + b : 0);
-        if constexpr (sizeof(T) == 8) cp_async16(dst + e, p, ok ? 16 : 0);
-        else cp_async8(dst + e, p, ok ? 8 : 0);
+// rest zero-filled) into shared memory, laid out [row][NB].  Thread tid owns
+// column tid % NB and rows tid / NB + k * (nt / NB).
+template <typename T, int NB, int NT, int TILE>
+__device__ __forceinline__ void tile_prefetch(V2<T> *dst, const V2<T> *__restrict__ src, const PassSpec &sp, int c0,
+                                              int tid) {
+    static_assert(NT % NB == 0, "threads must cover whole rows");
+    constexpr int RSTEP = NT / NB;
+    const int b = tid % NB;
+    const bool col_ok = c0 + b < sp.ncols;
+    const V2<T> *s = src + b;
+    V2<T> *d = dst + tid;
+#pragma unroll 4
+    for (int row = tid / NB; row * NB < TILE; row += RSTEP, d += NT) {
+        const bool ok = col_ok && sp.row_in.kept(row);
+        const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
+        const V2<T> *p = ok ? s + (long long)r * sp.s_row : src;
+        if constexpr (sizeof(T) == 8) cp_async16(d, p, ok ? 16 : 0);
+        else cp_async8(d, p, ok ? 8 : 0);
     }
 }
 
@@ -153,7 +160,7 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
         int fi, oc, o, c0;
         decode(it, fi, oc, o, c0);
         const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
-        tile_prefetch<T>(dst, src, sp, TILE, NB, c0, tid, NT);
+        tile_prefetch<T, NB, NT, TILE>(dst, src, sp, c0, tid);
     };
     prefetch(item, rawb[0]);
     cp_async_commit();
@@ -227,6 +234,40 @@ __device__ __forceinline__ void warp_line_fft(int lane, V2<T> *line, const V2<T>
             [&](int row, int, V v) { line[padded<T>(row)] = v; }, SyncWarp{});
         __syncwarp();
         warp_line_fft<T, N, SIGN, S + 1>(lane, line, tw);
+    }
+}
+
+// FFT of one padded line by one warp, ping-ponging between two line buffers
+// (a and b): stage s reads one and writes the other, so a lane holds one
+// radix-R butterfly at a time.  The result is in b after an odd number of
+// stages and in a after an even number (see pp_result).
+template <typename T, int N, int SIGN, int S = 0>
+__device__ __forceinline__ void warp_line_fft_pp(int lane, V2<T> *a, V2<T> *b, const V2<T> *tw) {
+    using V = V2<T>;
+    if constexpr (S < plan_nstages(N)) {
+        V *src = (S % 2 == 0) ? a : b;
+        V *dst = (S % 2 == 0) ? b : a;
+        fft_stage_stream<T, N, S, SIGN, 1, 32>(
+            lane, tw, [&](int row, int) -> V { return src[padded<T>(row)]; },
+            [&](int row, int, V v) { dst[padded<T>(row)] = v; });
+        __syncwarp();
+        warp_line_fft_pp<T, N, SIGN, S + 1>(lane, a, b, tw);
+    }
+}
+template <typename T, int N> __host__ __device__ constexpr bool pp_result_in_b() { return plan_nstages(N) % 2 == 1; }
+
+// In-place FFT of one padded line by the 64 threads of a warp pair that
+// synchronise on named barrier `bar` (t64 = 0..63).
+template <typename T, int N, int SIGN, int S = 0>
+__device__ __forceinline__ void pair_line_fft(int t64, V2<T> *line, const V2<T> *tw, int bar) {
+    using V = V2<T>;
+    if constexpr (S < plan_nstages(N)) {
+        const SyncNamed sync{bar, 64};
+        fft_stage<T, N, S, SIGN, 1, 64, true>(
+            t64, tw, [&](int row, int) -> V { return line[padded<T>(row)]; },
+            [&](int row, int, V v) { line[padded<T>(row)] = v; }, sync);
+        sync();
+        pair_line_fft<T, N, SIGN, S + 1>(t64, line, tw, bar);
     }
 }
 
@@ -304,12 +345,13 @@ k_zpass(FieldSet<T> f, long long nlines, int nz2, T scale, const V2<T> *__restri
 // One warp per input field; one block per line pair.
 template <typename T, int N> struct ZPCfg {
     static constexpr int LEN = padded_len<T>(N);   // padded line in the work area
-    __host__ __device__ static constexpr int work_bytes(int nph) {
-        return (nph * LEN * (int)sizeof(V2<T>) + 127) / 128 * 128;
+    // work area: one bank of nph lines, or two banks when the transforms ping-pong
+    __host__ __device__ static constexpr int work_bytes(int nph, bool pp) {
+        return ((pp ? 2 : 1) * nph * LEN * (int)sizeof(V2<T>) + 127) / 128 * 128;
     }
     // staging area: nraw fields x a line pair of ncp complex values each
-    __host__ __device__ static constexpr int pipe_bytes(int nph, int nraw, int ncp) {
-        return work_bytes(nph) + nraw * 2 * ncp * (int)sizeof(V2<T>) + 16;
+    __host__ __device__ static constexpr int pipe_bytes(int nph, int nraw, int ncp, bool pp) {
+        return work_bytes(nph, pp) + nraw * 2 * ncp * (int)sizeof(V2<T>) + 16;
     }
     static constexpr int SMEM_MAX = 227 * 1024;
 };
@@ -349,11 +391,12 @@ __device__ __forceinline__ void pack_c2r_combo(int lane, V2<T> *line, const ZRec
 }
 
 // R2C unpacking into a line pair of stride ncp: modes k <= N/2 are written,
-// columns beyond N/2 (padding of short lines) are set to zero.
+// columns beyond N/2 (padding of short lines) are set to zero.  Threads
+// t, t + nt, ... of the group share the work.
 template <typename T, int N>
-__device__ __forceinline__ void unpack_r2c_pad(int lane, const V2<T> *line, V2<T> *A, V2<T> *B, int ncp) {
+__device__ __forceinline__ void unpack_r2c_pad(int t, int nt, const V2<T> *line, V2<T> *A, V2<T> *B, int ncp) {
     using V = V2<T>;
-    for (int k = lane; k < ncp; k += 32) {
+    for (int k = t; k < ncp; k += nt) {
         if (k <= N / 2) {
             V zk = line[padded<T>(k)];
             V zm = line[padded<T>((N - k) % N)];
@@ -367,11 +410,12 @@ __device__ __forceinline__ void unpack_r2c_pad(int lane, const V2<T> *line, V2<T
 }
 
 // Pointwise products of one line pair held in the work area (real part =
-// line a, imaginary part = line b); results overwrite regions 0..4.
+// line a, imaginary part = line b); results go to regions 0..4 of `out`
+// (which may be the input bank: each point is read before it is written).
 // Regions: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3, 6 sx, 7 sy, 8 sz,
 // [9 cx, 10 cy, 11 cz], [12 c, 13 lap s].
 template <typename T, int N, int NPH>
-__device__ __forceinline__ void zphys_products(V2<T> *reg, T scale, T alpha) {
+__device__ __forceinline__ void zphys_products(const V2<T> *reg, V2<T> *out, T scale, T alpha) {
     using V = V2<T>;
     constexpr int LEN = ZPCfg<T, N>::LEN;
     constexpr bool has_c = NPH >= 12, has_al = NPH >= 14;
@@ -403,11 +447,11 @@ __device__ __forceinline__ void zphys_products(V2<T> *reg, T scale, T alpha) {
                 nc = adv;
             }
         }
-        reg[0 * LEN + pn] = n1;
-        reg[1 * LEN + pn] = n2;
-        reg[2 * LEN + pn] = n3;
-        reg[3 * LEN + pn] = ns;
-        if constexpr (has_c) reg[4 * LEN + pn] = nc;
+        out[0 * LEN + pn] = n1;
+        out[1 * LEN + pn] = n2;
+        out[2 * LEN + pn] = n3;
+        out[3 * LEN + pn] = ns;
+        if constexpr (has_c) out[4 * LEN + pn] = nc;
     }
 }
 
@@ -417,10 +461,12 @@ __device__ __forceinline__ void zphys_products(V2<T> *reg, T scale, T alpha) {
 // cp.async.bulk into a staging area while the current pair is transformed,
 // multiplied and written back; otherwise they are read from global memory
 // directly.  Warp q forms physical quantity q; the products are z-transformed
-// back and written over raw fields 0..nout-1 of the same pair.  A wait that
-// times out sets bit 0 of *err and the block stops.
-template <typename T, int N, int NPH, int NRAW>
-__global__ void __launch_bounds__(NPH * 32, 1)
+// back and written over raw fields 0..nout-1 of the same pair.  With PP the
+// line transforms ping-pong between two banks of lines (one butterfly per
+// lane at a time: fewer registers, more resident warps); otherwise they run
+// in place.  A wait that times out sets bit 0 of *err and the block stops.
+template <typename T, int N, int NPH, int NRAW, bool PP>
+__global__ void __launch_bounds__(NPH * 32, (PP && sizeof(T) == 4) ? 2 : 1)
 k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
         int ncp, int nkz, int pipe, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw,
         unsigned *__restrict__ err) {
@@ -430,9 +476,15 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
     const int rawf = 2 * ncp;
     const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *reg = reinterpret_cast<V *>(smem_raw);
-    V *raw = reinterpret_cast<V *>(smem_raw + C::work_bytes(NPH));
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + C::work_bytes(NPH) + NRAW * raw_bytes);
+    V *bankA = reinterpret_cast<V *>(smem_raw);
+    V *bankB = bankA + NPH * LEN;
+    V *raw = reinterpret_cast<V *>(smem_raw + C::work_bytes(NPH, PP));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + C::work_bytes(NPH, PP) + NRAW * raw_bytes);
+    // with PP: physical values land in bank B after an odd number of stages
+    constexpr bool PHYS_B = PP && pp_result_in_b<T, N>();
+    V *phys = PHYS_B ? bankB : bankA;           // physical quantities
+    V *prod = PP ? (PHYS_B ? bankA : bankB) : bankA;   // products (other bank with PP)
+    V *fres = PP ? (pp_result_in_b<T, N>() ? (PHYS_B ? bankB : bankA) : prod) : bankA;   // forward results
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     long long pair = blockIdx.x;
     if (pair >= npairs) return;   // uniform for the block
@@ -449,7 +501,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
     };
     if (pipe && threadIdx.x == 0) issue(pair);
     unsigned parity = 0;
-    V *line = reg + warp * LEN;
+    V *lineA = bankA + warp * LEN;
     const ZRecipe rc = zr.q[warp];
     for (; pair < npairs; pair += gridDim.x) {
         const V *a0, *a1;
@@ -467,7 +519,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
             a0 = f.p[rc.r[0]] + pair * rawf;
             a1 = rc.r[1] >= 0 ? f.p[rc.r[1]] + pair * rawf : nullptr;
         }
-        pack_c2r_combo<T, N>(lane, line, rc, a0, a1, ncp, nkz, dkz);
+        pack_c2r_combo<T, N>(lane, lineA, rc, a0, a1, ncp, nkz, dkz);
         __syncthreads();   // staging area (or the raw lines in global memory) consumed
         if (pipe) {
             const long long next = pair + gridDim.x;
@@ -477,14 +529,17 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
             }
         }
         __syncwarp();
-        warp_line_fft<T, N, +1>(lane, line, tw);   // every quantity to physical space
+        if constexpr (PP) warp_line_fft_pp<T, N, +1>(lane, lineA, bankB + warp * LEN, tw);
+        else warp_line_fft<T, N, +1>(lane, lineA, tw);   // every quantity to physical space
         __syncthreads();
-        zphys_products<T, N, NPH>(reg, scale, alpha);
+        zphys_products<T, N, NPH>(phys, prod, scale, alpha);
         __syncthreads();
         if (warp < nout) {   // z R2C of the products, written over raw fields 0..nout-1
-            warp_line_fft<T, N, -1>(lane, line, tw);
+            V *pl = prod + warp * LEN;
+            if constexpr (PP) warp_line_fft_pp<T, N, -1>(lane, pl, (prod == bankA ? bankB : bankA) + warp * LEN, tw);
+            else warp_line_fft<T, N, -1>(lane, pl, tw);
             V *d = f.p[warp] + pair * rawf;
-            unpack_r2c_pad<T, N>(lane, line, d, d + ncp, ncp);
+            unpack_r2c_pad<T, N>(lane, 32, fres + warp * LEN, d, d + ncp, ncp);
         }
         __syncthreads();   // work area reused by the next pair
     }
