@@ -129,24 +129,6 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-# stage -> (fields read, fields written) of one launch in the fused step, per the pass structure
-def stage_traffic(nphys: int, nnl: int, nf: int) -> dict:
-    return {
-        "x_inverse": (nf, nphys),          # state (dealiased, derivatives formed on load) -> quantities
-        "y_inverse": (nphys, nphys),
-        "z_physical": (nphys, nnl),        # physical products never leave the chip
-        "y_forward": (nnl, nnl),
-        "x_forward": (nnl, nnl),
-        "spectral_update": (nnl + 2 * nf, 2 * nf),   # nonlinear, state, history -> state, history
-    }
-
-
-def counts(n_scalars: int, alpha: float = 0.0):
-    nphys = 9 + (3 if n_scalars > 1 else 0) + (2 if (n_scalars > 1 and alpha != 0.0) else 0)
-    nnl = 3 + n_scalars
-    return nphys, nnl, 3 + n_scalars
-
-
 # ------------------------------------------------------------------ our arm
 def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None):
     """Time `steps` steps of one jet resident on `dev`; returns a dict."""
@@ -185,7 +167,7 @@ def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4,
     prof = ctx.profile_read()
     ctx.profile(False)
     out = dict(ms=ms, launches=launches, clocks=clk.summary(), stats=stats, profile=prof,
-               field_bytes=ctx.field_bytes())
+               field_bytes=ctx.field_bytes(), stage_bytes=ctx.stage_bytes())
     del st, hi
     ctx.close()
     torch.cuda.empty_cache()
@@ -277,14 +259,12 @@ def ours(args):
                "h2d_bytes_per_step": int(e["h2d"]), "d2h_bytes_per_step": int(e["d2h"]),
                "steps_per_call": E2E_STEPS_PER_CALL,
                "call": "gnss_run_host: pinned host state in, steps, per-step statistics and state out"}
-    # roofline of the dominant kernel (stage of the fused step with the largest device time)
-    nphys, nnl, nf = counts(1)
-    traffic = stage_traffic(nphys, nnl, nf)
+    # roofline of the dominant kernel (stage of the fused step with the largest device time);
+    # algorithmic bytes per launch come from the library's own layout (gnss_stage_bytes)
     prof = leg["profile"]
     dom = max(prof, key=lambda k: prof[k][0])
     t_ms, nl = prof[dom]
-    rd, wr = traffic[dom]
-    alg = (rd + wr) * leg["field_bytes"]
+    alg = leg["stage_bytes"][dom]
     peaks = measured_peaks()
     achieved = alg / (t_ms / nl * 1e-3) / 1e9
     tr_file = ROOT / "profiles" / "traffic.json"
@@ -293,11 +273,13 @@ def ours(args):
         tj = json.loads(tr_file.read_text())
         key = f"{args.precision}:{n}:{dom}"
         if key in tj:
-            traffic_meas = tj[key]
+            traffic_meas = tj[key]["bytes_per_launch"]
     roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic_meas,
                 "algorithmic_bytes": int(alg), "peak_source": peaks["source"] + " (burst copy)",
-                "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()}}
+                "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()},
+                "stages_gbs": {k: round(leg["stage_bytes"][k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
+                               for k, v in prof.items()}}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()

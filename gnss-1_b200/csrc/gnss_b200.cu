@@ -643,6 +643,23 @@ gnss_status gnss_check(gnss_ctx *c, void *stream) {
     return GNSS_OK;
 }
 
+gnss_status gnss_stage_bytes(const gnss_ctx *c, double *bytes) {
+    if (!c || !bytes) return GNSS_ERR_INVALID;
+    const double e = (double)c->elem;
+    const int nf = 3 + c->cfg.n_scalars;
+    const double nkx = c->kx_keep.count(), nky = c->ky_keep.count();
+    const double box = nky * nkx * c->nkz;                    // kept modes of one state field
+    const double pe = (double)c->p_elems, qe = (double)c->q_elems;
+    const double re = nky * nkx * c->ncp;                     // x-forward output
+    bytes[0] = e * (c->n_xin * box + c->n_xout * pe);          // x inverse
+    bytes[1] = e * (c->n_xout * pe + c->n_raw * qe);           // y inverse
+    bytes[2] = e * (c->n_raw * qe + c->nnl * qe);              // z physical
+    bytes[3] = e * (c->nnl * qe + c->nnl * pe);                // y forward
+    bytes[4] = e * (c->nnl * pe + c->nnl * re);                // x forward
+    bytes[5] = e * (c->nnl * box + 4.0 * nf * box);            // update: nl, state, hist in; state, hist out
+    return GNSS_OK;
+}
+
 gnss_status gnss_profile_enable(gnss_ctx *c, int on) {
     if (!c) return GNSS_ERR_INVALID;
     c->profiling = on != 0;

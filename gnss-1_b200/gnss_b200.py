@@ -88,6 +88,7 @@ _SIGS = {
     "gnss_check": [_VP, _VP],
     "gnss_forward_noalloc": [ctypes.POINTER(GnssConfig), _VP, _VP],
     "gnss_profile_enable": [_VP, ctypes.c_int],
+    "gnss_stage_bytes": [_VP, ctypes.POINTER(ctypes.c_double)],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
 }
 _RESTYPES = {
@@ -315,6 +316,12 @@ class Context:
     # -- instrumentation ------------------------------------------------------
     def launch_count(self) -> int:
         return int(self.lib.gnss_launch_count(self._h))
+
+    def stage_bytes(self) -> dict:
+        """Algorithmic HBM bytes of one launch of each stage of the step."""
+        b = (ctypes.c_double * len(STAGE_NAMES))()
+        self._ck(self.lib.gnss_stage_bytes(self._h, b), "gnss_stage_bytes")
+        return {k: float(b[i]) for i, k in enumerate(STAGE_NAMES)}
 
     def profile(self, on: bool) -> None:
         self._ck(self.lib.gnss_profile_enable(self._h, int(bool(on))), "gnss_profile_enable")

@@ -178,6 +178,10 @@ gnss_status gnss_check(gnss_ctx *ctx, void *stream);
  * (arrays of GNSS_NSTAGES entries), and clears the record. */
 #define GNSS_NSTAGES 6
 long long gnss_launch_count(const gnss_ctx *ctx);
+/* Algorithmic HBM bytes of one launch of each stage of gnss_step (the
+ * compulsory reads and writes of the pruned layouts; GNSS_NSTAGES doubles),
+ * for roofline accounting. */
+gnss_status gnss_stage_bytes(const gnss_ctx *ctx, double *bytes);
 gnss_status gnss_profile_enable(gnss_ctx *ctx, int on);
 gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 
