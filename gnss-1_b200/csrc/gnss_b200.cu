@@ -37,6 +37,7 @@ struct gnss_ctx {
     KeepMap kx_keep{}, ky_keep{};
     int nkz = 0, ncp = 0;
     size_t p_elems = 0, q_elems = 0;
+    long long n_sphere = 0;                       // kept-box modes inside the dealiasing sphere
     int n_xin = 0;                                // x-inverse inputs (state fields; s twice with alpha)
     signed char xvar_in[6]{}, xvar_n[6]{}, xvar_mul[6][2]{}, xvar_out[6][2]{};
     signed char yvar_n[MAXF]{}, yvar_mul[MAXF][2]{}, yvar_out[MAXF][2]{};
@@ -534,8 +535,16 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
     }
     {
         StageTimer t(c, s, 5);
-        const long long nmodes = (long long)c->ky_keep.count() * c->kx_keep.count() * c->nkz;
-        k_update<T><<<grid_for(nmodes, 256), 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc);
+        // one warp per kept (ky, kx) row; 8 blocks of 8 warps per SM
+        const long long nrows = (long long)c->ky_keep.count() * c->kx_keep.count();
+        const int full_rows = (uc.scheme == GNSS_SCHEME_CNAB2 && uc.euler) ? 1 : 0;
+        const long long nblk = std::min<long long>((nrows + 7) / 8, 8LL * c->nsm);
+        if (uc.scheme == GNSS_SCHEME_CNAB2)
+            k_update<T, GNSS_SCHEME_CNAB2><<<(unsigned)nblk, 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz,
+                                                                        c->ncp, uc, full_rows);
+        else
+            k_update<T, GNSS_SCHEME_RK3IF><<<(unsigned)nblk, 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz,
+                                                                        c->ncp, uc, full_rows);
         LAUNCH_CK(c);
     }
     return GNSS_OK;
@@ -656,7 +665,9 @@ gnss_status gnss_stage_bytes(const gnss_ctx *c, double *bytes) {
     bytes[2] = e * (c->n_raw * qe + c->nnl * qe);              // z physical
     bytes[3] = e * (c->nnl * qe + c->nnl * pe);                // y forward
     bytes[4] = e * (c->nnl * pe + c->nnl * re);                // x forward
-    bytes[5] = e * (c->nnl * box + 4.0 * nf * box);            // update: nl, state, hist in; state, hist out
+    const double sph = (double)c->n_sphere;
+    bytes[5] = e * (c->nnl * sph + 4.0 * nf * sph);            // update (after the first step): nl, state, hist in;
+                                                               // state, hist out, inside the sphere
     return GNSS_OK;
 }
 
@@ -807,6 +818,21 @@ static void set_layout(gnss_ctx *c) {
     c->ncp = (c->nkz + 15) / 16 * 16;
     c->p_elems = (size_t)g.nx * c->ky_keep.count() * c->ncp;
     c->q_elems = (size_t)g.nx * g.ny * c->ncp;
+    // modes of the kept box inside the dealiasing sphere (the ones k_update touches after the first step)
+    auto wn = [](int i, int n, double dk) { return (i < n / 2) ? dk * (double)i : dk * ((double)i - (double)n); };
+    c->n_sphere = 0;
+    for (int yc = 0; yc < c->ky_keep.count(); ++yc) {
+        const double k2 = wn(c->ky_keep.expand(yc), g.ny, g.dky);
+        for (int xc = 0; xc < c->kx_keep.count(); ++xc) {
+            const double k1 = wn(c->kx_keep.expand(xc), g.nx, g.dkx);
+            const double t = k1 * k1 + k2 * k2;
+            for (int z = 0; z < c->nkz; ++z) {
+                const double k3 = wn(z, g.nz, g.dkz);
+                if (t + k3 * k3 > g.kmax2) break;
+                ++c->n_sphere;
+            }
+        }
+    }
 }
 
 gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out) {

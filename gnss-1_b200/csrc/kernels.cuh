@@ -557,95 +557,117 @@ struct UpdCoef {
     int substep;      // IF-RK3: 0, 1, 2 (substep 0 ignores the history input)
 };
 
-// One thread per spectral mode (grid-stride).  The arithmetic follows
-// makeRHS / deAlias / timestep / update (solver.cu:461-657) with the divisions
-// by k^2 and by (1 + dt k^2/(2 num)) done once as reciprocals.
-// Modes are enumerated in the kept box (kept ky, kept kx, kz < nkz); nl is
-// the compact [kyc][kxc][ncp] layout of the forward passes; state and hist
-// use the reference layout.  Modes outside the box are neither read nor
-// written: they stay zero once the state has been dealiased.
-template <typename T>
+// One warp per (ky, kx) row of the kept box, lanes along kz.  The arithmetic
+// follows makeRHS / deAlias / timestep / update (solver.cu:461-657) with the
+// divisions by k^2 and by (1 + dt k^2/(2 num)) done once as reciprocals.
+// Rows are enumerated in the kept box (kept ky, kept kx); nl is the compact
+// [kyc][kxc][ncp] layout of the forward passes; state and hist use the
+// reference layout.  Along kz the unmasked modes of a row form a prefix
+// (k^2 grows with kz), so the warp stops at the first chunk of 32 that is
+// masked throughout.  With full_rows the masked modes of the box (kz < nkz)
+// are written as zero instead (the first step of a run: it clears whatever
+// the history held there); modes outside the box are never touched.  Every
+// load of a mode is issued before its first store.
+template <typename T, int SCHEME>
 __global__ void __launch_bounds__(256)
 k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
          const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
-         UpdCoef c) {
+         UpdCoef c, int full_rows) {
     using V = V2<T>;
     const int nkx = kx_keep.count(), nky = ky_keep.count();
-    const long long nmodes = (long long)nky * nkx * nkz;
-    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nmodes;
-         m += (long long)gridDim.x * blockDim.x) {
-        const int kzi = (int)(m % nkz);
-        const long long t = m / nkz;
-        const int kxc = (int)(t % nkx);
-        const int kyc = (int)(t / nkx);
+    const int nrows = nky * nkx;
+    const int lane = threadIdx.x & 31;
+    const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+    const bool read_hist = (SCHEME == 0) ? !c.euler : (c.substep > 0);
+    const int nf = c.nf;
+    for (int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); row < nrows; row += nwarp) {
+        const int kyc = row / nkx, kxc = row - kyc * nkx;
         const int kxi = kx_keep.expand(kxc), kyi = ky_keep.expand(kyc);
-        const long long idx = ((long long)kyi * g.nx + kxi) * g.nz2 + kzi;      // state / hist
-        const long long jdx = ((long long)kyc * nkx + kxc) * ncp + kzi;         // nonlinear term
-        const double k1 = wavenum(kxi, g.nx, g.dkx), k2 = wavenum(kyi, g.ny, g.dky), k3 = wavenum(kzi, g.nz, g.dkz);
-        const double ksq = ksq3(k1, k2, k3);
-        const bool masked = ksq > g.kmax2;
-        const bool zero_mode = (kxi == 0 && kyi == 0 && kzi == 0);
-        double R[5][2];
-        // makeRHS: (k k^T / k^2 - I) N for the velocity, -N for the scalars,
-        // zero at k = 0; then deAlias(rhs) (solver.cu:756)
-        if (zero_mode || masked) {
+        const double k1 = wavenum(kxi, g.nx, g.dkx), k2 = wavenum(kyi, g.ny, g.dky);
+        const long long base = ((long long)kyi * g.nx + kxi) * g.nz2;   // state / hist
+        const long long jbase = (long long)row * ncp;                     // nonlinear term
+        for (int k0 = 0; k0 < nkz; k0 += 32) {
+            const int kzi = k0 + lane;
+            const bool inrow = kzi < nkz;
+            const double k3 = wavenum(kzi, g.nz, g.dkz);
+            const double ksq = ksq3(k1, k2, k3);
+            const bool masked = ksq > g.kmax2;
+            if (!full_rows && __all_sync(0xffffffffu, masked || !inrow)) break;
+            if (!inrow) continue;
+            const long long idx = base + kzi, jdx = jbase + kzi;
+            if (masked) {
+                // deAlias of the state and of the right-hand side (solver.cu:36, 756)
+                if (full_rows) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) R[q][0] = R[q][1] = 0.0;
-        } else {
-            const double ik = 1.0 / ksq;
-            const V a = nl.p[0][jdx], b = nl.p[1][jdx], cc = nl.p[2][jdx];
-            const double pr = (k1 * (double)a.x + k2 * (double)b.x + k3 * (double)cc.x) * ik;   // k . N / k^2
-            const double pi = (k1 * (double)a.y + k2 * (double)b.y + k3 * (double)cc.y) * ik;
-            R[0][0] = k1 * pr - (double)a.x;
-            R[0][1] = k1 * pi - (double)a.y;
-            R[1][0] = k2 * pr - (double)b.x;
-            R[1][1] = k2 * pi - (double)b.y;
-            R[2][0] = k3 * pr - (double)cc.x;
-            R[2][1] = k3 * pi - (double)cc.y;
+                    for (int q = 0; q < 5; ++q) {
+                        if (q < nf) {
+                            state.p[q][idx] = V{T(0), T(0)};
+                            hist.p[q][idx] = V{T(0), T(0)};
+                        }
+                    }
+                }
+                continue;
+            }
+            V a[5], f[5], h[5];
 #pragma unroll
-            for (int q = 3; q < 5; ++q) {
-                if (q < c.nf) {
-                    const V s = nl.p[q][jdx];
-                    R[q][0] = -(double)s.x;
-                    R[q][1] = -(double)s.y;
-                } else {
-                    R[q][0] = R[q][1] = 0.0;
+            for (int q = 0; q < 5; ++q) {
+                a[q] = V{T(0), T(0)};
+                f[q] = V{T(0), T(0)};
+                h[q] = V{T(0), T(0)};
+                if (q < nf) {
+                    a[q] = nl.p[q][jdx];
+                    f[q] = state.p[q][idx];
+                    if (read_hist) h[q] = hist.p[q][idx];
                 }
             }
-        }
+            // makeRHS: (k k^T / k^2 - I) N for the velocity, -N for the scalars,
+            // zero at k = 0 (solver.cu:461-521)
+            double R[5][2];
+            if (kxi == 0 && kyi == 0 && kzi == 0) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            if (q >= c.nf) break;
-            const V fv = state.p[q][idx];
-            const double fr = masked ? 0.0 : (double)fv.x, fi = masked ? 0.0 : (double)fv.y;
-            if (c.scheme == 0) {
-                // eulerKernel_mgpu / adamsBashforthKernel_mgpu (solver.cu:547-585)
-                const double hk = c.hnum[q] * ksq;
-                const double a = 1.0 - hk;
-                const double ib = 1.0 / (1.0 + hk);
-                double nr, ni;
-                if (c.euler) {
-                    nr = (a * fr + c.dt * R[q][0]) * ib;
-                    ni = (a * fi + c.dt * R[q][1]) * ib;
-                } else {
-                    const V ro = hist.p[q][idx];
-                    nr = (a * fr + c.dt * (1.5 * R[q][0] - 0.5 * (double)ro.x)) * ib;
-                    ni = (a * fi + c.dt * (1.5 * R[q][1] - 0.5 * (double)ro.y)) * ib;
-                }
-                state.p[q][idx] = V{(T)nr, (T)ni};
-                hist.p[q][idx] = V{(T)R[q][0], (T)R[q][1]};   // updateKernel_mgpu (solver.cu:618-637)
+                for (int q = 0; q < 5; ++q) R[q][0] = R[q][1] = 0.0;
             } else {
-                const double E = exp(-c.nu[q] * ksq * c.alph * c.dt);
-                double hr = 0.0, hi = 0.0;
-                if (c.substep > 0) {
-                    const V h = hist.p[q][idx];
-                    hr = (double)h.x;
-                    hi = (double)h.y;
+                const double ik = 1.0 / ksq;
+                const double pr = (k1 * (double)a[0].x + k2 * (double)a[1].x + k3 * (double)a[2].x) * ik;
+                const double pi = (k1 * (double)a[0].y + k2 * (double)a[1].y + k3 * (double)a[2].y) * ik;
+                R[0][0] = k1 * pr - (double)a[0].x;
+                R[0][1] = k1 * pi - (double)a[0].y;
+                R[1][0] = k2 * pr - (double)a[1].x;
+                R[1][1] = k2 * pi - (double)a[1].y;
+                R[2][0] = k3 * pr - (double)a[2].x;
+                R[2][1] = k3 * pi - (double)a[2].y;
+#pragma unroll
+                for (int q = 3; q < 5; ++q) {
+                    R[q][0] = -(double)a[q].x;
+                    R[q][1] = -(double)a[q].y;
                 }
-                const double nr = E * (fr + c.gam * c.dt * R[q][0] + hr);
-                const double ni = E * (fi + c.gam * c.dt * R[q][1] + hi);
-                state.p[q][idx] = V{(T)nr, (T)ni};
-                hist.p[q][idx] = V{(T)(c.zet_next * c.dt * E * R[q][0]), (T)(c.zet_next * c.dt * E * R[q][1])};
+            }
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                if (q >= nf) break;
+                const double fr = (double)f[q].x, fi = (double)f[q].y;
+                if constexpr (SCHEME == 0) {
+                    // eulerKernel_mgpu / adamsBashforthKernel_mgpu (solver.cu:547-585)
+                    const double hk = c.hnum[q] * ksq;
+                    const double am = 1.0 - hk;
+                    const double ib = 1.0 / (1.0 + hk);
+                    double nr, ni;
+                    if (c.euler) {
+                        nr = (am * fr + c.dt * R[q][0]) * ib;
+                        ni = (am * fi + c.dt * R[q][1]) * ib;
+                    } else {
+                        nr = (am * fr + c.dt * (1.5 * R[q][0] - 0.5 * (double)h[q].x)) * ib;
+                        ni = (am * fi + c.dt * (1.5 * R[q][1] - 0.5 * (double)h[q].y)) * ib;
+                    }
+                    state.p[q][idx] = V{(T)nr, (T)ni};
+                    hist.p[q][idx] = V{(T)R[q][0], (T)R[q][1]};   // updateKernel_mgpu (solver.cu:618-637)
+                } else {
+                    const double E = exp(-c.nu[q] * ksq * c.alph * c.dt);
+                    const double nr = E * (fr + c.gam * c.dt * R[q][0] + (double)h[q].x);
+                    const double ni = E * (fi + c.gam * c.dt * R[q][1] + (double)h[q].y);
+                    state.p[q][idx] = V{(T)nr, (T)ni};
+                    hist.p[q][idx] = V{(T)(c.zet_next * c.dt * E * R[q][0]), (T)(c.zet_next * c.dt * E * R[q][1])};
+                }
             }
         }
     }

@@ -137,8 +137,12 @@ gnss_status gnss_colloid_advection(gnss_ctx *ctx, const void *u, const void *v, 
  * wavenumber along any axis exceeds the truncation radius are neither read
  * nor written, so they must be zero on entry (gnss_dealias does that, as the
  * reference does once before its loop, main.cu:156, and at the start of
- * every step, solver.cu:704); within the kept box the step applies the
- * spherical mask itself and leaves exact zeros outside the sphere.
+ * every step, solver.cu:704).  Within the kept box the spherical mask is
+ * applied on input, so masked modes of the state never enter the step.  The
+ * Euler step (euler != 0) writes exact zeros to the masked modes of state and
+ * history inside the box; the other steps update only the modes inside the
+ * sphere and leave the masked ones as they are (zero, for a dealiased state
+ * and a history written by an earlier step).
  * state: spectral u, v, w, s (and c).  hist: for GNSS_SCHEME_CNAB2 the
  * previous RHS (the reference's rhs_old; read when euler == 0, always
  * written); unused (may be NULL) for GNSS_SCHEME_RK3IF.  euler selects the
