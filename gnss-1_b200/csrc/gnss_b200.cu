@@ -12,6 +12,7 @@
 
 #include "gnss_b200.h"
 #include "kernels.cuh"
+#include "zreg.cuh"
 
 using namespace gnss;
 
@@ -37,6 +38,7 @@ struct gnss_ctx {
     KeepMap kx_keep{}, ky_keep{};
     int nkz = 0, ncp = 0;
     size_t p_elems = 0, q_elems = 0;
+    int zvariant = GNSS_ZVARIANT_AUTO;            // z kernel choice (gnss_set_option)
     long long n_sphere = 0;                       // kept-box modes inside the dealiasing sphere
     int n_xin = 0;                                // x-inverse inputs (state fields; s twice with alpha)
     signed char xvar_in[6]{}, xvar_n[6]{}, xvar_mul[6][2]{}, xvar_out[6][2]{};
@@ -214,9 +216,47 @@ template <typename T, int N> struct Launch {
             return zphys_k<NPH, NRAW, true>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
         return zphys_k<NPH, NRAW, false>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
     }
+    // register-resident line transforms (N = 256, 512) when their shared memory fits
+    template <int NPH, int NRAW>
+    static cudaError_t zreg_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
+                              T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s) {
+        if constexpr (N == 256 || N == 512) {
+            const int smem = ZRCfg<T, N>::smem_bytes(NPH, NRAW, ncp);
+            if (smem > ZPCfg<T, N>::SMEM_MAX) return cudaErrorNotSupported;
+            auto kern = k_zreg<T, N, NPH, NRAW>;
+            cudaError_t e = prep_smem(kern, smem);
+            if (e != cudaSuccess) return e;
+            const int per_sm = blocks_per_sm(kern, NPH * 32, smem);
+            const long long npairs = nlines / 2;
+            long long grid = (long long)per_sm * nsm;
+            if (grid > npairs) grid = npairs;
+            kern<<<(unsigned)grid, NPH * 32, smem, s>>>(f, zr, nout, npairs, ncp, nkz, scale, alpha, dkz,
+                                                         reinterpret_cast<const V2<T> *>(tw), err);
+            return cudaGetLastError();
+        } else {
+            (void)f; (void)zr; (void)nout; (void)nlines; (void)ncp; (void)nkz; (void)scale; (void)alpha; (void)dkz;
+            (void)tw; (void)err; (void)nsm; (void)s;
+            return cudaErrorNotSupported;
+        }
+    }
+    static bool zreg_fits(int nph, int nraw, int ncp) {
+        if constexpr (N == 256 || N == 512)
+            return ZRCfg<T, N>::smem_bytes(nph, nraw, ncp) <= ZPCfg<T, N>::SMEM_MAX;
+        else
+            return false;
+    }
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
-                             unsigned *err, int nsm, cudaStream_t s) {
+                             unsigned *err, int nsm, cudaStream_t s, int zvariant) {
+        if (zvariant != GNSS_ZVARIANT_STAGED && zreg_fits(nph, nraw, ncp)) {
+            if (nph == 9 && nraw == 10)
+                return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            if (nph == 12 && nraw == 13)
+                return zreg_k<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            if (nph == 14 && nraw == 14)
+                return zreg_k<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            return cudaErrorInvalidValue;
+        }
         if (nph == 9 && nraw == 10)
             return zphys_n<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
         if (nph == 12 && nraw == 13)
@@ -258,9 +298,9 @@ static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfield
 template <typename T>
 static cudaError_t launch_zphys(int n, const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                                 long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
-                                unsigned *err, int nsm, cudaStream_t s) {
+                                unsigned *err, int nsm, cudaStream_t s, int zvariant) {
     GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::zphys(f, zr, nph, nraw, nout, nlines, ncp, nkz, scale, alpha, dkz, tw,
-                                                      err, nsm, s)));
+                                                      err, nsm, s, zvariant)));
 }
 template <typename T> static int pass_nb(int n) {
     switch (n) {
@@ -519,7 +559,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
     {
         StageTimer t(c, s, 2);
         CK(c, launch_zphys<T>(g.nz, Q, c->zrec, c->n_phys, nq, nnl, nlines, c->ncp, c->nkz, scale, (T)c->cfg.alpha,
-                              g.dkz, c->tw[2], c->d_err, c->nsm, s));
+                              g.dkz, c->tw[2], c->d_err, c->nsm, s, c->zvariant));
     }
     {
         StageTimer t(c, s, 3);
@@ -669,6 +709,26 @@ gnss_status gnss_stage_bytes(const gnss_ctx *c, double *bytes) {
     bytes[5] = e * (c->nnl * sph + 4.0 * nf * sph);            // update (after the first step): nl, state, hist in;
                                                                // state, hist out, inside the sphere
     return GNSS_OK;
+}
+
+gnss_status gnss_set_option(gnss_ctx *c, int key, int value) {
+    if (!c) return GNSS_ERR_INVALID;
+    if (key == GNSS_OPT_ZVARIANT) {
+        if (value < GNSS_ZVARIANT_AUTO || value > GNSS_ZVARIANT_STAGED)
+            return fail(c, GNSS_ERR_INVALID, "bad z variant %d", value);
+        c->zvariant = value;
+        return GNSS_OK;
+    }
+    return fail(c, GNSS_ERR_INVALID, "unknown option %d", key);
+}
+
+gnss_status gnss_get_option(const gnss_ctx *c, int key, int *value) {
+    if (!c || !value) return GNSS_ERR_INVALID;
+    if (key == GNSS_OPT_ZVARIANT) {
+        *value = c->zvariant;
+        return GNSS_OK;
+    }
+    return GNSS_ERR_INVALID;
 }
 
 gnss_status gnss_profile_enable(gnss_ctx *c, int on) {

@@ -1,0 +1,349 @@
+// zreg.cuh -- fused z pass with register-resident line transforms (N = 256, 512).
+//
+// Same work as k_zphys (kz factors and vorticity combinations, C2R of every
+// physical quantity of a line pair, the pointwise products, R2C of the
+// products), with a different line transform: a warp holds its line in
+// registers, E = N/32 elements per lane, and runs the length-N DFT as
+//   N = E * 32,   32 = E * G   (G = 32/E lanes per group)
+//   step A: E-point DFT in registers over elements lane + 32 m, twiddle
+//           W_N^(lane k1);
+//   one transpose through a padded per-warp scratch;
+//   step B: E-point DFT in registers, twiddle W_32^(j k2'), and a G-point
+//           DFT across the lanes of a group with shuffles.
+// A line therefore crosses shared memory once per transform (instead of once
+// per radix-8 stage), the C2R packing is done while loading the registers,
+// and the twiddles of step A are products of four table powers.  Physical
+// values are exchanged between warps through one bank of lines; two block
+// barriers per line pair.
+#pragma once
+#include "kernels.cuh"
+
+namespace gnss {
+
+// cos(2 pi e / 32) for e = 0..8; other angles by symmetry.
+__host__ __device__ constexpr double cos32_tab(int e) {
+    return e == 0   ? 1.0
+           : e == 1 ? 0.98078528040323044912618223613424
+           : e == 2 ? 0.92387953251128675612818318939679
+           : e == 3 ? 0.83146961230254523707878837761791
+           : e == 4 ? 0.70710678118654752440084436210485
+           : e == 5 ? 0.55557023301960222474283081394853
+           : e == 6 ? 0.38268343236508977172845998403040
+           : e == 7 ? 0.19509032201612826784828486847702
+                    : 0.0;
+}
+__host__ __device__ constexpr double cos32(int e) {
+    e = ((e % 32) + 32) % 32;
+    return e <= 8 ? cos32_tab(e) : e <= 16 ? -cos32_tab(16 - e) : e <= 24 ? -cos32_tab(e - 16) : cos32_tab(32 - e);
+}
+__host__ __device__ constexpr double sin32(int e) { return cos32(e - 8); }
+
+// v * exp(S 2 pi i e / 32) with compile-time e
+template <int S, int EXP, typename V> __device__ __forceinline__ V mul_w32(V v) {
+    using T = decltype(v.x);
+    constexpr int e = ((EXP % 32) + 32) % 32;
+    if constexpr (e == 0) {
+        return v;
+    } else if constexpr (e == 8) {
+        return mul_si<S>(v);
+    } else if constexpr (e == 16) {
+        return V{-v.x, -v.y};
+    } else if constexpr (e == 24) {
+        return mul_si<-S>(v);
+    } else {
+        constexpr T c = (T)cos32(e);
+        constexpr T s = (T)((double)S * sin32(e));
+        return V{v.x * c - v.y * s, v.x * s + v.y * c};
+    }
+}
+
+// 16-point DFT in natural order: n = 4 n1 + n2, k = k1 + 4 k2.
+template <int S, typename V> __device__ __forceinline__ void dft16(V *v) {
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4<S>(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+    // v[4 k1 + n2] = y[n2][k1]; twiddle W_16^(n2 k1) = W_32^(2 n2 k1)
+    v[5] = mul_w32<S, 2>(v[5]);
+    v[9] = mul_w32<S, 4>(v[9]);
+    v[13] = mul_w32<S, 6>(v[13]);
+    v[6] = mul_w32<S, 4>(v[6]);
+    v[10] = mul_w32<S, 8>(v[10]);
+    v[14] = mul_w32<S, 12>(v[14]);
+    v[7] = mul_w32<S, 6>(v[7]);
+    v[11] = mul_w32<S, 12>(v[11]);
+    v[15] = mul_w32<S, 18>(v[15]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<S>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // v[4 k1 + k2] = X[k1 + 4 k2] -> natural order
+    V t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) t[k1 + 4 * k2] = v[4 * k1 + k2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+template <int S, typename V> struct Dft<16, S, V> {
+    static __device__ __forceinline__ void run(V *v) { dft16<S>(v); }
+};
+
+template <typename T, int N> struct ZRCfg {
+    static constexpr int E = N / 32;                    // elements per lane
+    static constexpr int G = 32 / E;                    // lanes per group in step B
+    static constexpr int S = 32 + G;                    // transpose row stride (conflict-free both ways)
+    static constexpr int SCR = E * S;                   // transpose scratch per warp
+    static constexpr int LOGE = E == 16 ? 4 : 3;        // table powers W^(lane 2^b), b < LOGE
+    static constexpr int PADP = (sizeof(T) == 4 && E == 8) ? 8 : 0;   // line padding per 64 entries
+    static constexpr int PL = N + PADP * (N / 64);      // physical line length in shared memory
+    __host__ __device__ static constexpr int pidx(int n) { return n + PADP * (n >> 6); }
+    static_assert(E == 8 || E == 16, "register z transform serves N = 256 and 512");
+    static_assert(SCR >= PL, "scratch holds a padded line");
+    __host__ __device__ static constexpr int smem_bytes(int nph, int nraw, int ncp) {
+        return (LOGE * 32 + nph * PL + nph * SCR + nraw * 2 * ncp) * (int)sizeof(V2<T>) + 16;
+    }
+};
+
+// Output slot of a lane group member after the G-point cross-lane DFT.
+template <int G> __device__ __forceinline__ int zr_sigma(int j) {
+    return G == 2 ? j : ((j >> 1) | ((j & 1) << 1));
+}
+
+template <int S, int Q, int G, typename V> __device__ __forceinline__ V zr_tw32(V v, int j) {
+    if constexpr (G == 2) {
+        const V y = mul_w32<S, Q>(v);
+        return j ? y : v;
+    } else {
+        const V y1 = mul_w32<S, Q>(v), y2 = mul_w32<S, 2 * Q>(v), y3 = mul_w32<S, 3 * Q>(v);
+        return j == 0 ? v : j == 1 ? y1 : j == 2 ? y2 : y3;
+    }
+}
+template <int S, int G, int Q, int E, typename V> __device__ __forceinline__ void zr_tw32_all(V *x, int j) {
+    if constexpr (Q < E) {
+        x[Q] = zr_tw32<S, Q, G>(x[Q], j);
+        zr_tw32_all<S, G, Q + 1, E>(x, j);
+    }
+}
+
+template <typename V> __device__ __forceinline__ V shfl_xor_v(V v, int m) {
+    return V{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
+}
+
+// Length-N DFT of one line held by a warp.  On entry x[m] is element
+// lane + 32 m; on return x[q] is element k1 + E q + E^2 zr_sigma(j) of the
+// transform, with k1 = lane / G, j = lane % G.  scr: this warp's scratch;
+// tws: table powers tws[32 b + l] = exp(-2 pi i l 2^b / N).
+template <typename T, int N, int SIGN>
+__device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<T> *tws) {
+    using V = V2<T>;
+    using Z = ZRCfg<T, N>;
+    constexpr int E = Z::E, G = Z::G, S = Z::S;
+    Dft<E, SIGN, V>::run(x);
+    {
+        V w[E];
+#pragma unroll
+        for (int b = 0; b < Z::LOGE; ++b) {
+            V t = tws[32 * b + lane];
+            if (SIGN > 0) t.y = -t.y;
+            w[1 << b] = t;
+        }
+        w[3] = cmul(w[1], w[2]);
+        w[5] = cmul(w[1], w[4]);
+        w[6] = cmul(w[2], w[4]);
+        w[7] = cmul(w[3], w[4]);
+        if constexpr (E == 16) {
+#pragma unroll
+            for (int i = 1; i < 8; ++i) w[8 + i] = cmul(w[i], w[8]);
+        }
+#pragma unroll
+        for (int k1 = 1; k1 < E; ++k1) x[k1] = cmul(x[k1], w[k1]);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) scr[k1 * S + lane] = x[k1];
+    __syncwarp();
+    const int k1 = lane / G, j = lane % G;
+#pragma unroll
+    for (int l = 0; l < E; ++l) x[l] = scr[k1 * S + G * l + j];
+    __syncwarp();
+    Dft<E, SIGN, V>::run(x);
+    zr_tw32_all<SIGN, G, 1, E>(x, j);
+    if constexpr (G == 2) {
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const V p = shfl_xor_v(x[q], 1);
+            x[q] = j == 0 ? cadd(x[q], p) : csub(p, x[q]);
+        }
+    } else {
+        const int j0 = j & 1, j1 = j >> 1;
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const V p = shfl_xor_v(x[q], 2);
+            V c = j1 == 0 ? cadd(x[q], p) : csub(p, x[q]);
+            if (j0 && j1) c = mul_si<SIGN>(c);
+            const V p2 = shfl_xor_v(c, 1);
+            x[q] = j0 == 0 ? cadd(c, p2) : csub(p2, c);
+        }
+    }
+}
+
+// Line index held in x[q] after zr_fft.
+template <typename T, int N> __device__ __forceinline__ int zr_out_index(int lane, int q) {
+    using Z = ZRCfg<T, N>;
+    return lane / Z::G + Z::E * q + Z::E * Z::E * zr_sigma<Z::G>(lane % Z::G);
+}
+
+// C2R packing (as pack_c2r_combo) straight into the registers of zr_fft:
+// x[m] = Z_n, n = lane + 32 m.
+template <typename T, int N>
+__device__ __forceinline__ void zr_pack(int lane, V2<T> *x, const ZRecipe rc, const V2<T> *a0, const V2<T> *a1,
+                                        int ncp, int nkz, double dkz) {
+    using V = V2<T>;
+    constexpr int E = ZRCfg<T, N>::E;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int n = lane + 32 * m;
+        const bool lo = 2 * n <= N;
+        const int k = lo ? n : N - n;
+        V z = V{T(0), T(0)};
+        if (k < nkz) {
+            const T kz = (T)wavenum(k, N, dkz);
+            V a = a0[k], b = a0[ncp + k];
+            if (rc.ikz[0]) { a = V{-kz * a.y, kz * a.x}; b = V{-kz * b.y, kz * b.x}; }
+            if (rc.sgn[0] < 0) { a = V{-a.x, -a.y}; b = V{-b.x, -b.y}; }
+            if (a1) {
+                V c = a1[k], d = a1[ncp + k];
+                if (rc.ikz[1]) { c = V{-kz * c.y, kz * c.x}; d = V{-kz * d.y, kz * d.x}; }
+                if (rc.sgn[1] < 0) { a = csub(a, c); b = csub(b, d); }
+                else { a = cadd(a, c); b = cadd(b, d); }
+            }
+            if (k == 0 || 2 * k == N) { a.y = T(0); b.y = T(0); }
+            z = lo ? V{a.x - b.y, a.y + b.x} : V{a.x + b.y, b.x - a.y};
+        }
+        x[m] = z;
+    }
+}
+
+// Product f of the physical quantities at elements lane + 32 m (the input
+// layout of zr_fft).  Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3, 6 sx, 7 sy,
+// 8 sz, [9 cx, 10 cy, 11 cz], [12 c, 13 lap s]; products as zphys_products.
+template <typename T, int N, int NPH>
+__device__ __forceinline__ void zr_products(int f, int lane, V2<T> *x, const V2<T> *phys, T alpha) {
+    using V = V2<T>;
+    using Z = ZRCfg<T, N>;
+    constexpr int E = Z::E, PL = Z::PL;
+    constexpr bool has_c = NPH >= 12, has_al = NPH >= 14;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const V *p = phys + Z::pidx(lane + 32 * m);
+        auto q = [&](int i) -> V { return p[i * PL]; };
+        V r;
+        if (f == 0) {          // (w x u)_x  (crossProductKernel_mgpu, solver.cu:139-164)
+            const V o2 = q(4), w = q(2), o3 = q(5), v = q(1);
+            r = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
+        } else if (f == 1) {   // (w x u)_y
+            const V o1 = q(3), w = q(2), o3 = q(5), u = q(0);
+            r = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
+        } else if (f == 2) {   // (w x u)_z
+            const V o1 = q(3), v = q(1), o2 = q(4), u = q(0);
+            r = V{o1.x * v.x - o2.x * u.x, o1.y * v.y - o2.y * u.y};
+        } else if (f == 3) {   // u . grad s  (dotKernel_mgpu, solver.cu:342-356)
+            const V u = q(0), v = q(1), w = q(2), sx = q(6), sy = q(7), sz = q(8);
+            r = V{u.x * sx.x + v.x * sy.x + w.x * sz.x, u.y * sx.y + v.y * sy.y + w.y * sz.y};
+        } else {               // colloid term (colloidAdvectionKernel_mgpu, solver.cu:374-388)
+            r = V{T(0), T(0)};
+            if constexpr (has_c) {
+                const V u = q(0), v = q(1), w = q(2), cx = q(9), cy = q(10), cz = q(11);
+                const V adv = V{u.x * cx.x + v.x * cy.x + w.x * cz.x, u.y * cx.y + v.y * cy.y + w.y * cz.y};
+                if constexpr (has_al) {
+                    const V sx = q(6), sy = q(7), sz = q(8), cc = q(12), ls = q(13);
+                    const V dr = V{ls.x * cc.x + cx.x * sx.x + cy.x * sy.x + cz.x * sz.x,
+                                   ls.y * cc.y + cx.y * sx.y + cy.y * sy.y + cz.y * sz.y};
+                    r = V{alpha * dr.x + adv.x, alpha * dr.y + adv.y};
+                } else {
+                    r = adv;
+                }
+            }
+        }
+        x[m] = r;
+    }
+}
+
+// Persistent: block b handles line pairs b, b + gridDim.x, ...; warp q forms
+// physical quantity q.  The raw lines of the next pair arrive by
+// cp.async.bulk (CTA-local, no multicast) while the current pair is
+// processed; a wait that times out sets bit 0 of *err and the block stops.
+template <typename T, int N, int NPH, int NRAW>
+__global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? 2 : 1)
+k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
+       int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err) {
+    using V = V2<T>;
+    using Z = ZRCfg<T, N>;
+    constexpr int E = Z::E, PL = Z::PL, SCR = Z::SCR;
+    const int rawf = 2 * ncp;
+    const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tws = reinterpret_cast<V *>(smem_raw);
+    V *phys = tws + Z::LOGE * 32;
+    V *scr_all = phys + NPH * PL;
+    V *raw = scr_all + NPH * SCR;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(raw + NRAW * rawf);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    long long pair = blockIdx.x;
+    if (pair >= npairs) return;   // uniform for the block
+    for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](long long p) {
+        mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
+        for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+    };
+    if (threadIdx.x == 0) issue(pair);
+    unsigned parity = 0;
+    const ZRecipe rc = zr.q[warp];
+    V *scr = scr_all + warp * SCR;
+    V *myphys = phys + warp * PL;
+    for (; pair < npairs; pair += gridDim.x) {
+        const bool ok = mbar_wait_bounded(bar, parity);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(err, 1u);
+            mbar_wait_bounded(bar, parity);   // let an overdue copy land before leaving
+            return;
+        }
+        parity ^= 1u;
+        V x[E];
+        zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp, nkz,
+                      dkz);
+        __syncthreads();   // staging consumed; the previous pair's products are read
+        if (threadIdx.x == 0 && pair + gridDim.x < npairs) {
+            fence_proxy_async_smem();
+            issue(pair + gridDim.x);
+        }
+        zr_fft<T, N, +1>(lane, x, scr, tws);
+#pragma unroll
+        for (int q = 0; q < E; ++q) myphys[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
+        __syncthreads();   // every physical quantity on chip
+        if (warp < nout) {   // z R2C of product `warp`, written over raw field `warp` of the pair
+            zr_products<T, N, NPH>(warp, lane, x, phys, alpha);
+            zr_fft<T, N, -1>(lane, x, scr, tws);
+#pragma unroll
+            for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = x[q];
+            __syncwarp();
+            V *d = f.p[warp] + pair * rawf;
+            for (int k = lane; k < ncp; k += 32) {
+                V A = V{T(0), T(0)}, B = V{T(0), T(0)};
+                if (2 * k <= N) {
+                    const V zk = scr[Z::pidx(k)];
+                    const V zm = scr[Z::pidx((N - k) % N)];
+                    A = V{T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
+                    B = V{T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
+                }
+                d[k] = A;
+                d[ncp + k] = B;
+            }
+            __syncwarp();   // scratch reused by the next transform
+        }
+    }
+}
+
+}  // namespace gnss

@@ -32,6 +32,10 @@ GNSS_SCHEME_RK3IF = 1
 GNSS_FP64 = 0
 GNSS_FP32 = 1
 GNSS_NSTATS = 7
+GNSS_OPT_ZVARIANT = 0
+GNSS_ZVARIANT_AUTO = 0
+GNSS_ZVARIANT_REGISTER = 1
+GNSS_ZVARIANT_STAGED = 2
 STAT_NAMES = ("ke", "vrms2", "eps", "chi_s", "chi_c", "var_s", "var_c")
 SUPPORTED_SIZES = (8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512)
 
@@ -89,6 +93,8 @@ _SIGS = {
     "gnss_forward_noalloc": [ctypes.POINTER(GnssConfig), _VP, _VP],
     "gnss_profile_enable": [_VP, ctypes.c_int],
     "gnss_stage_bytes": [_VP, ctypes.POINTER(ctypes.c_double)],
+    "gnss_set_option": [_VP, ctypes.c_int, ctypes.c_int],
+    "gnss_get_option": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
 }
 _RESTYPES = {
@@ -316,6 +322,14 @@ class Context:
     # -- instrumentation ------------------------------------------------------
     def launch_count(self) -> int:
         return int(self.lib.gnss_launch_count(self._h))
+
+    def set_option(self, key: int, value: int) -> None:
+        self._ck(self.lib.gnss_set_option(self._h, key, value), "gnss_set_option")
+
+    def get_option(self, key: int) -> int:
+        v = ctypes.c_int()
+        self._ck(self.lib.gnss_get_option(self._h, key, ctypes.byref(v)), "gnss_get_option")
+        return v.value
 
     def stage_bytes(self) -> dict:
         """Algorithmic HBM bytes of one launch of each stage of the step."""

@@ -189,6 +189,21 @@ gnss_status gnss_stage_bytes(const gnss_ctx *ctx, double *bytes);
 gnss_status gnss_profile_enable(gnss_ctx *ctx, int on);
 gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 
+/* Kernel variant options of a context (the knobs the autotuner sets; no
+ * counterpart in the reference, which has one cuFFT plan per size).
+ * GNSS_OPT_ZVARIANT picks the kernel of the fused z stage:
+ *   GNSS_ZVARIANT_AUTO      register-resident line transforms where they
+ *                           exist (N = 256, 512) and fit, else staged;
+ *   GNSS_ZVARIANT_REGISTER  the same as AUTO (a request, not a guarantee);
+ *   GNSS_ZVARIANT_STAGED    per-stage line transforms through shared memory.
+ * Every variant computes the same step to round-off. */
+#define GNSS_OPT_ZVARIANT 0
+#define GNSS_ZVARIANT_AUTO 0
+#define GNSS_ZVARIANT_REGISTER 1
+#define GNSS_ZVARIANT_STAGED 2
+gnss_status gnss_set_option(gnss_ctx *ctx, int key, int value);
+gnss_status gnss_get_option(const gnss_ctx *ctx, int key, int *value);
+
 /* Forward transform that allocates nothing.  No counterpart in the
  * reference.  For callers that may not allocate device memory: code running
  * under a memory manager that owns the whole device (a framework's caching
