@@ -133,8 +133,10 @@ def measured_peaks() -> dict:
 def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None):
     """Time `steps` steps of one jet resident on `dev`; returns a dict."""
     cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
-    init = G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
-    ctx = G.Context(n, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme, device=dev)
+    nx, ny, nz = (n, n, n) if isinstance(n, int) else n
+    init = G.jet_initial_state(nx, ny, nz, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
+    ctx = G.Context(nx=nx, ny=ny, nz=nz, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme,
+                    device=dev)
     st = [torch.from_numpy(a.astype(cdt)).to(f"cuda:{dev}") for a in init]
     del init
     hi = [torch.zeros_like(st[0]) for _ in st] if scheme == G.GNSS_SCHEME_CNAB2 else None
@@ -201,6 +203,128 @@ def run_e2e(G, torch, n, precision, scheme, calls, dev):
                 d2h=(state_bytes + E2E_STEPS_PER_CALL * G.GNSS_NSTATS * 8) / E2E_STEPS_PER_CALL)
 
 
+def run_error_vs_fp64(G, torch, n, steps, dev) -> dict:
+    """Per-field relative L2 of the mixed-precision state against the FP64 state
+    after `steps` steps from the same initial state (both on the device)."""
+    init = G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
+    res = {}
+    for prec in (G.GNSS_FP64, G.GNSS_FP32):
+        cdt = np.complex128 if prec == G.GNSS_FP64 else np.complex64
+        with G.Context(n, re=RE, sc=SC, dt=DT, n_scalars=1, precision=prec, device=dev) as ctx:
+            st = [torch.from_numpy(a.astype(cdt)).to(f"cuda:{dev}") for a in init]
+            hi = [torch.zeros_like(st[0]) for _ in st]
+            ctx.de_alias(st)
+            for k in range(steps):
+                ctx.solver_ps(st, hi, euler=(k == 0))
+            ctx.check()
+            res[prec] = st
+            del hi
+    ref, got = res[G.GNSS_FP64], res[G.GNSS_FP32]
+    errs = [float((g.to(torch.complex128) - r).norm() / r.norm()) for g, r in zip(got, ref)]
+    del res, ref, got
+    torch.cuda.empty_cache()
+    return {"steps": steps, "rel_l2_per_field": dict(zip(("u", "v", "w", "s"), [float(f"{e:.3e}") for e in errs])),
+            "max": float(f"{max(errs):.3e}"), "tolerance": 1e-5}
+
+
+# ensemble of BASELINE's batching form: 16 x 64^3, 8 x 96^3, 6 x 128^3, 2 x 192^3
+ENSEMBLE_SIZES = [64] * 16 + [96] * 8 + [128] * 6 + [192] * 2
+
+
+def run_ensemble(G, torch, dev, steps, branches=8) -> dict:
+    rng = np.random.default_rng(4)
+    res = rng.uniform(500.0, 4000.0, len(ENSEMBLE_SIZES))
+    scs = rng.choice([0.7, 1.0, 2.0], len(ENSEMBLE_SIZES))
+    cfgs = [G.make_config(n, re=float(r), sc=float(sc), dt=1e-3, precision=G.GNSS_FP32, device=dev)
+            for n, r, sc in zip(ENSEMBLE_SIZES, res, scs)]
+    points = float(sum(n ** 3 for n in ENSEMBLE_SIZES))
+    with G.Ensemble(cfgs, n_branches=branches) as ens:
+        t0 = time.perf_counter()
+        choices = ens.autotune(3)
+        t_tune = time.perf_counter() - t0
+        for i, n in enumerate(ENSEMBLE_SIZES):
+            f = G.jet_initial_state(n, n_scalars=1, seed=i, noise_kmax=NOISE_K, amp=AMP, dtype=np.complex64)
+            ens.upload(i, G.pack_state(f))
+        stream = torch.cuda.current_stream(dev)
+        chunk = 50
+        ens.step(1 + chunk)        # first (Euler) step and graph capture, untimed
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clk:
+            e0.record(stream)
+            for _ in range(steps // chunk):
+                ens.step(chunk)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / (steps // chunk * chunk)
+        lps = ens.launches_per_step()
+        ke = [ens.stats(i)["ke"] for i in (0, 16, 24, 30)]
+    assert all(math.isfinite(k) for k in ke)
+    return {"value": round(points / (ms * 1e-3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(ms, 4),
+            "steps": steps // chunk * chunk, "members": len(cfgs), "points_per_step": int(points),
+            "workload": "16x64^3 + 8x96^3 + 6x128^3 + 2x192^3 jets, Re ~ U[500,4000], Sc in {0.7,1,2}, seeds 0-31, "
+                        "FP32, dt 1e-3, cnab2",
+            "graph": f"{chunk} steps of all 32 members per CUDA graph launch, {branches} branches",
+            "gpu_launches_per_step": lps, "autotune_s": round(t_tune, 2),
+            "autotune_choices": {str(n): int(choices[ENSEMBLE_SIZES.index(n)]) for n in sorted(set(ENSEMBLE_SIZES))},
+            "clocks": clk.summary()}
+
+
+SERVE_SIZES = (64, 96, 128, 192, 256)
+
+
+def run_serving(G, dev, duration_s=15.0, rate=4.0) -> dict:
+    """Poisson arrivals of jet runs into the continuous-batching server; latency
+    is submission to completion on the server's clock."""
+    rng = np.random.default_rng(5)
+    pool = {}
+    for n in SERVE_SIZES:
+        for ns in (1, 2):
+            f = G.jet_initial_state(n, n_scalars=ns, seed=n + ns, noise_kmax=NOISE_K, amp=AMP, dtype=np.complex64)
+            pool[(n, ns)] = G.pack_state(f)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration_s:
+            break
+        arrivals.append(t)
+    reqs = []
+    for a in arrivals:
+        n = int(rng.choice(SERVE_SIZES))
+        ns = int(rng.integers(1, 3))
+        re = float(rng.uniform(500.0, 5000.0))
+        steps = int(rng.integers(100, 2001))
+        reqs.append((a, G.make_config(n, re=re, sc=0.7, sc_c=1.0, dt=5e-4, n_scalars=ns, precision=G.GNSS_FP32,
+                                      device=dev), pool[(n, ns)], steps))
+    budget = 150 << 30
+    ids = []
+    with G.Server(budget_bytes=budget, max_active=64, steps_per_launch=25, device=dev) as srv:
+        t0 = time.perf_counter()
+        for a, cfg, st, steps in reqs:
+            d = t0 + a - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(cfg, st, steps))
+        lat, first, last = [], None, 0.0
+        for rid in ids:
+            srv.wait(rid, timeout=1800.0)
+            _, _, tm = srv.result(rid)
+            lat.append(tm[2] - tm[0])
+            first = tm[0] if first is None else min(first, tm[0])
+            last = max(last, tm[2])
+        rep = srv.report()
+    lat = np.array(lat)
+    return {"requests": len(ids), "arrival_rate_per_s": rate, "arrival_window_s": duration_s,
+            "p50_s": round(float(np.percentile(lat, 50)), 3), "p99_s": round(float(np.percentile(lat, 99)), 3),
+            "mean_s": round(float(lat.mean()), 3),
+            "value": round(rep["point_steps"] / (last - first) / 1e6, 3), "unit": UNIT,
+            "completed": rep["completed"], "failed": rep["failed"], "active_max": rep["active_max"],
+            "budget_gb": budget / 2 ** 30, "reserved_max_gb": round(rep["bytes_reserved_max"] / 2 ** 30, 2),
+            "workload": "Poisson arrivals, N in {64,96,128,192,256}^3, Re ~ U[500,5000], 100-2000 steps, "
+                        "1-2 scalars, FP32, dt 5e-4; 25 steps per graph launch, 64 slots, 150 GB budget"}
+
+
 def cpu_baseline(n_sample=256, steps=2) -> dict:
     """The CPU oracle (same scheme and parameters) on all host cores, bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -240,19 +364,20 @@ def ours(args):
     prec = G.GNSS_FP32 if args.precision == "mixed" else G.GNSS_FP64
     scheme = G.GNSS_SCHEME_CNAB2 if args.scheme == "cnab2" else G.GNSS_SCHEME_RK3IF
     n = args.n
-    leg = run_leg(G, torch, n, prec, scheme, args.steps, args.warmup, dev, barrier=barrier)
+    shape = tuple(int(v) for v in args.grid.split("x")) if args.grid else (n, n, n)
+    leg = run_leg(G, torch, shape, prec, scheme, args.steps, args.warmup, dev, barrier=barrier)
     ms = leg["ms"] if red is None else red(leg["ms"])
-    pts = float(n) ** 3
+    pts = float(shape[0] * shape[1] * shape[2])
     value = replica_value(pts, ms, ws)
     fp64 = None
     if prec == G.GNSS_FP32 and not args.no_fp64_leg:
-        l64 = run_leg(G, torch, n, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier)
+        l64 = run_leg(G, torch, shape, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier)
         ms64 = l64["ms"] if red is None else red(l64["ms"])
         fp64 = {"value": round(replica_value(pts, ms64, ws), 3), "ms_per_step": round(ms64, 4),
                 "mixed_over_fp64": round(ms64 / ms, 3),
                 "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in l64["profile"].items()}}
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not args.grid:
         e = run_e2e(G, torch, n, prec, scheme, args.e2e_calls, dev)
         ms_call = e["ms_call"] if red is None else red(e["ms_call"])
         e2e = {"value": round(replica_value(pts * E2E_STEPS_PER_CALL, ms_call, ws), 3), "unit": UNIT,
@@ -271,7 +396,7 @@ def ours(args):
     traffic_meas = None
     if tr_file.exists():
         tj = json.loads(tr_file.read_text())
-        key = f"{args.precision}:{n}:{dom}"
+        key = f"{args.precision}:{args.grid or n}:{dom}"
         if key in tj:
             traffic_meas = tj[key]["bytes_per_launch"]
     roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
@@ -280,6 +405,19 @@ def ours(args):
                 "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()},
                 "stages_gbs": {k: round(leg["stage_bytes"][k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
                                for k, v in prof.items()}}
+    err = None
+    if prec == G.GNSS_FP32 and not args.no_error_check and not args.grid:
+        err = run_error_vs_fp64(G, torch, n, args.error_steps, dev)
+    ens = None
+    if not args.no_ensemble and not args.grid:
+        ens = run_ensemble(G, torch, dev, args.ensemble_steps)
+        if red is not None:
+            ens["value"] = round(ws * ens["points_per_step"] / (red(ens["ms_per_step"]) * 1e-3) / 1e6, 3)
+    serve = None
+    if not args.no_serve and not args.grid:
+        serve = run_serving(G, dev, args.serve_seconds)
+        if red is not None:   # whole-job throughput: every rank served its own stream
+            serve["p99_s"] = red(serve["p99_s"])
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -293,13 +431,14 @@ def ours(args):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if prec == G.GNSS_FP32 else "f64", "data": "synthetic",
-        "config": {"workload": f"temporal jet {n}^3, 1 scalar, Re {RE:g}, Sc {SC}, dt {DT:g}, "
+        "config": {"workload": f"temporal jet {'x'.join(map(str, shape)) if args.grid else f'{n}^3'}, "
+                               f"1 scalar, Re {RE:g}, Sc {SC}, dt {DT:g}, "
                                f"noise |k|<={NOISE_K:g} rms {AMP}, 2/3 dealias, {args.scheme}",
                    "grid": n, "precision": args.precision, "scheme": args.scheme,
                    "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (>= 0.5 GB per field); no flush"},
         "gpu_launches": leg["launches"], "clocks": leg["clocks"], "e2e": e2e, "roofline": roofline,
-        "cpu_baseline": cpu, "fp64": fp64,
+        "cpu_baseline": cpu, "fp64": fp64, "error_vs_fp64": err, "ensemble": ens, "serving": serve,
         "stats_after": {k: leg["stats"][k] for k in ("ke", "eps", "chi_s", "var_s")},
     }
     print(json.dumps(line), flush=True)
@@ -348,12 +487,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--grid", default=None, help="NXxNYxNZ instead of n^3 (profiling workloads; no e2e leg)")
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--scheme", choices=("cnab2", "rk3if"), default="cnab2")
     ap.add_argument("--e2e-calls", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-leg", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-error-check", action="store_true")
+    ap.add_argument("--error-steps", type=int, default=100)
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=15.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("bench.py: at least 3 warm-up steps are required", file=sys.stderr)

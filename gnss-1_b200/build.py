@@ -15,8 +15,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-SOURCES = [HERE / "csrc" / "gnss_b200.cu"]
-DEPS = SOURCES + [HERE / "csrc" / "fft.cuh", HERE / "csrc" / "kernels.cuh", ROOT / "include" / "gnss_b200.h"]
+SOURCES = [HERE / "csrc" / "gnss_b200.cu", HERE / "csrc" / "batch.cpp"]
+DEPS = sorted((HERE / "csrc").glob("*")) + [ROOT / "include" / "gnss_b200.h"]
 OUT = HERE / "libgnss_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -1,0 +1,725 @@
+// batch.cpp -- ensembles and the serving loop, built on the C ABI of
+// gnss_b200.h.
+//
+// Ensemble: many independent jets (uneven grids, Reynolds and Schmidt numbers)
+// stepped together.  Members are spread over a few non-blocking streams; the
+// steps of all members are captured once into one CUDA graph (one branch per
+// stream, members of a branch one after another on a shared scratch buffer)
+// and replayed, so a block of steps of the whole ensemble is one launch.
+//
+// Server: continuous batching.  Submitted requests wait in arrival order; a
+// scheduler thread admits them as soon as an active slot and enough of the
+// device-memory budget are free, and advances every active request on its own
+// stream in chunks of steps (one graph launch per chunk).  Device memory of a
+// request (state, history, scratch) is stream-ordered (cudaMallocAsync /
+// cudaFreeAsync), so admissions and completions never synchronise the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "gnss_b200.h"
+
+namespace {
+
+size_t elem_bytes(const gnss_config &c) { return c.precision == GNSS_FP64 ? 16 : 8; }
+size_t field_bytes_of(const gnss_config &c) {
+    return (size_t)c.nx * c.ny * (c.nz / 2 + 1) * elem_bytes(c);
+}
+int nfields_of(const gnss_config &c) { return 3 + c.n_scalars; }
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+gnss_fields fields_at(void *base, size_t fb, int nf) {
+    void *p[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < nf; ++q) p[q] = static_cast<char *>(base) + (size_t)q * fb;
+    return gnss_fields{p[0], p[1], p[2], p[3], p[4]};
+}
+
+struct Member {
+    gnss_config cfg{};
+    gnss_ctx *ctx = nullptr;
+    void *buf = nullptr;   // state (nf fields) then history (nf fields)
+    gnss_fields state{}, hist{};
+    int branch = 0;
+    long long launches_per_step = 0;
+};
+
+}  // namespace
+
+// ====================================================================== ensemble
+struct gnss_ensemble {
+    int device = 0;
+    std::vector<Member> m;
+    int nbranch = 1;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> ev_join;
+    std::vector<void *> branch_scratch;
+    cudaEvent_t ev_fork = nullptr;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int g_steps = 0;
+    long long steps_done = 0;
+};
+
+static void ensemble_free(gnss_ensemble *e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    cudaDeviceSynchronize();
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    for (Member &mb : e->m) {
+        if (mb.ctx) gnss_destroy(mb.ctx);
+        if (mb.buf) cudaFree(mb.buf);
+    }
+    for (void *p : e->branch_scratch) if (p) cudaFree(p);
+    for (cudaStream_t s : e->streams) if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t ev : e->ev_join) if (ev) cudaEventDestroy(ev);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->cap) cudaStreamDestroy(e->cap);
+    delete e;
+}
+
+gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n, int nbranch, gnss_ensemble **out) {
+    if (!cfgs || !out || n < 1 || nbranch < 1) return GNSS_ERR_INVALID;
+    *out = nullptr;
+    const int dev = cfgs[0].device;
+    for (int i = 1; i < n; ++i)
+        if (cfgs[i].device != dev) return GNSS_ERR_INVALID;   // one device per ensemble
+    if (cudaSetDevice(dev) != cudaSuccess) return GNSS_ERR_CUDA;
+    gnss_ensemble *e = new gnss_ensemble;
+    e->device = dev;
+    e->nbranch = std::min(nbranch, n);
+    e->m.resize(n);
+    gnss_status st = GNSS_OK;
+    for (int i = 0; i < n && st == GNSS_OK; ++i) {
+        Member &mb = e->m[i];
+        mb.cfg = cfgs[i];
+        st = gnss_create(&cfgs[i], &mb.ctx);
+        if (st) break;
+        const size_t fb = field_bytes_of(mb.cfg);
+        const int nf = nfields_of(mb.cfg);
+        if (cudaMalloc(&mb.buf, 2 * nf * fb) != cudaSuccess || cudaMemset(mb.buf, 0, 2 * nf * fb) != cudaSuccess) {
+            cudaGetLastError();
+            mb.buf = nullptr;
+            st = GNSS_ERR_NOMEM;
+            break;
+        }
+        mb.state = fields_at(mb.buf, fb, nf);
+        mb.hist = fields_at(static_cast<char *>(mb.buf) + nf * fb, fb, nf);
+    }
+    if (st) {
+        ensemble_free(e);
+        return st;
+    }
+    // longest processing time first: each member (by points) to the least-loaded branch
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    auto pts = [&](int i) { return (double)e->m[i].cfg.nx * e->m[i].cfg.ny * e->m[i].cfg.nz; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pts(a) > pts(b); });
+    std::vector<double> load(e->nbranch, 0.0);
+    std::vector<size_t> need(e->nbranch, 0);
+    for (int i : order) {
+        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        e->m[i].branch = b;
+        load[b] += pts(i);
+        need[b] = std::max(need[b], round256(gnss_scratch_bytes(e->m[i].ctx)));
+    }
+    e->streams.assign(e->nbranch, nullptr);
+    e->ev_join.assign(e->nbranch, nullptr);
+    e->branch_scratch.assign(e->nbranch, nullptr);
+    for (int b = 0; b < e->nbranch && st == GNSS_OK; ++b) {
+        if (cudaStreamCreateWithFlags(&e->streams[b], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e->ev_join[b], cudaEventDisableTiming) != cudaSuccess)
+            st = GNSS_ERR_CUDA;
+        else if (need[b] && cudaMalloc(&e->branch_scratch[b], need[b]) != cudaSuccess)
+            st = GNSS_ERR_NOMEM;
+    }
+    if (!st && (cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking) != cudaSuccess))
+        st = GNSS_ERR_CUDA;
+    for (int i = 0; i < n && !st; ++i) {
+        const int b = e->m[i].branch;
+        st = gnss_attach_scratch(e->m[i].ctx, e->branch_scratch[b], need[b]);
+    }
+    if (st) {
+        cudaGetLastError();
+        ensemble_free(e);
+        return st;
+    }
+    *out = e;
+    return GNSS_OK;
+}
+
+gnss_status gnss_ensemble_destroy(gnss_ensemble *e) {
+    if (!e) return GNSS_ERR_INVALID;
+    ensemble_free(e);
+    return GNSS_OK;
+}
+
+int gnss_ensemble_size(const gnss_ensemble *e) { return e ? (int)e->m.size() : 0; }
+
+gnss_status gnss_ensemble_member(gnss_ensemble *e, int i, gnss_ctx **ctx, gnss_fields *state, gnss_fields *hist) {
+    if (!e || i < 0 || i >= (int)e->m.size()) return GNSS_ERR_INVALID;
+    if (ctx) *ctx = e->m[i].ctx;
+    if (state) *state = e->m[i].state;
+    if (hist) *hist = e->m[i].hist;
+    return GNSS_OK;
+}
+
+gnss_status gnss_ensemble_upload(gnss_ensemble *e, int i, const void *host_state, void *stream) {
+    if (!e || i < 0 || i >= (int)e->m.size() || !host_state) return GNSS_ERR_INVALID;
+    if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
+    Member &mb = e->m[i];
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t fb = field_bytes_of(mb.cfg);
+    const int nf = nfields_of(mb.cfg);
+    if (cudaMemcpyAsync(mb.buf, host_state, nf * fb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemsetAsync(static_cast<char *>(mb.buf) + nf * fb, 0, nf * fb, s) != cudaSuccess)
+        return GNSS_ERR_CUDA;
+    void *f[5] = {mb.state.u, mb.state.v, mb.state.w, mb.state.s, mb.state.c};
+    for (int q = 0; q < nf; ++q) {
+        gnss_status st = gnss_dealias(mb.ctx, f[q], stream);
+        if (st) return st;
+    }
+    return GNSS_OK;
+}
+
+gnss_status gnss_ensemble_download(gnss_ensemble *e, int i, void *host_state, void *stream) {
+    if (!e || i < 0 || i >= (int)e->m.size() || !host_state) return GNSS_ERR_INVALID;
+    if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
+    Member &mb = e->m[i];
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t bytes = nfields_of(mb.cfg) * field_bytes_of(mb.cfg);
+    if (cudaMemcpyAsync(host_state, mb.buf, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return GNSS_ERR_CUDA;
+    return GNSS_OK;
+}
+
+long long gnss_ensemble_launches_per_step(const gnss_ensemble *e) {
+    if (!e) return 0;
+    long long s = 0;
+    for (const Member &mb : e->m) s += mb.launches_per_step;
+    return s;
+}
+
+// Every member's steps in branch order on the branch streams, forked from and
+// joined back into stream `s`.
+static gnss_status ensemble_issue(gnss_ensemble *e, int n_steps, int euler_first, cudaStream_t s) {
+    if (cudaEventRecord(e->ev_fork, s) != cudaSuccess) return GNSS_ERR_CUDA;
+    for (int b = 0; b < e->nbranch; ++b)
+        if (cudaStreamWaitEvent(e->streams[b], e->ev_fork, 0) != cudaSuccess) return GNSS_ERR_CUDA;
+    for (Member &mb : e->m) {
+        const cudaStream_t bs = e->streams[mb.branch];
+        for (int k = 0; k < n_steps; ++k) {
+            const long long l0 = gnss_launch_count(mb.ctx);
+            gnss_status st = gnss_step(mb.ctx, &mb.state, &mb.hist, (euler_first && k == 0) ? 1 : 0, bs);
+            if (st) return st;
+            mb.launches_per_step = gnss_launch_count(mb.ctx) - l0;
+        }
+    }
+    for (int b = 0; b < e->nbranch; ++b) {
+        if (cudaEventRecord(e->ev_join[b], e->streams[b]) != cudaSuccess) return GNSS_ERR_CUDA;
+        if (cudaStreamWaitEvent(s, e->ev_join[b], 0) != cudaSuccess) return GNSS_ERR_CUDA;
+    }
+    return GNSS_OK;
+}
+
+static gnss_status ensemble_capture(gnss_ensemble *e, int n_steps) {
+    if (e->gexec) {
+        cudaGraphExecDestroy(e->gexec);
+        e->gexec = nullptr;
+    }
+    if (cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeRelaxed) != cudaSuccess) return GNSS_ERR_CUDA;
+    gnss_status st = ensemble_issue(e, n_steps, 0, e->cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->cap, &g);
+    if (st == GNSS_OK && ce != cudaSuccess) st = GNSS_ERR_CUDA;
+    if (st == GNSS_OK && cudaGraphInstantiate(&e->gexec, g, 0) != cudaSuccess) st = GNSS_ERR_CUDA;
+    if (g) cudaGraphDestroy(g);
+    if (st) {
+        cudaGetLastError();
+        e->gexec = nullptr;
+        return st;
+    }
+    e->g_steps = n_steps;
+    return GNSS_OK;
+}
+
+gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream) {
+    if (!e || n_steps < 0) return GNSS_ERR_INVALID;
+    if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (n_steps == 0) return GNSS_OK;
+    if (e->steps_done == 0) {   // the first step of a run (Euler for the reference scheme), launched directly
+        gnss_status st = ensemble_issue(e, 1, 1, s);
+        if (st) return st;
+        e->steps_done = 1;
+        if (--n_steps == 0) return GNSS_OK;
+    }
+    if (!e->gexec || e->g_steps != n_steps) {
+        gnss_status st = ensemble_capture(e, n_steps);
+        if (st) return st;
+    }
+    if (cudaGraphLaunch(e->gexec, s) != cudaSuccess) return GNSS_ERR_CUDA;
+    e->steps_done += n_steps;
+    return GNSS_OK;
+}
+
+gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
+    if (!e || steps < 1) return GNSS_ERR_INVALID;
+    if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
+    using Key = std::tuple<int, int, int, int, int, int>;
+    std::map<Key, int> best;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    gnss_status st = GNSS_OK;
+    const int variants[2] = {GNSS_ZVARIANT_AUTO, GNSS_ZVARIANT_STAGED};
+    for (Member &mb : e->m) {
+        const Key k{mb.cfg.nx, mb.cfg.ny, mb.cfg.nz, mb.cfg.precision, mb.cfg.n_scalars, mb.cfg.scheme};
+        if (best.count(k)) continue;
+        const cudaStream_t bs = e->streams[mb.branch];
+        float tbest = 0.f;
+        int vbest = GNSS_ZVARIANT_AUTO;
+        for (int v : variants) {
+            if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v))) break;
+            if ((st = gnss_step(mb.ctx, &mb.state, &mb.hist, 1, bs))) break;   // warm-up
+            cudaEventRecord(t0, bs);
+            for (int i = 0; i < steps && !st; ++i) st = gnss_step(mb.ctx, &mb.state, &mb.hist, 0, bs);
+            cudaEventRecord(t1, bs);
+            if (st) break;
+            cudaEventSynchronize(t1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, t0, t1);
+            if (v == variants[0] || ms < tbest) {
+                tbest = ms;
+                vbest = v;
+            }
+        }
+        if (st) break;
+        best[k] = vbest;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (st) return st;
+    for (size_t i = 0; i < e->m.size(); ++i) {
+        Member &mb = e->m[i];
+        const int v = best[Key{mb.cfg.nx, mb.cfg.ny, mb.cfg.nz, mb.cfg.precision, mb.cfg.n_scalars, mb.cfg.scheme}];
+        if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v))) return st;
+        if (choices) choices[i] = v;
+        const size_t fb = field_bytes_of(mb.cfg);
+        if (cudaMemset(mb.buf, 0, 2 * nfields_of(mb.cfg) * fb) != cudaSuccess) return GNSS_ERR_CUDA;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return GNSS_ERR_CUDA;
+    if (e->gexec) {
+        cudaGraphExecDestroy(e->gexec);
+        e->gexec = nullptr;
+    }
+    e->steps_done = 0;
+    return GNSS_OK;
+}
+
+// ====================================================================== server
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    long long id = 0;
+    gnss_config cfg{};
+    int n_steps = 0;
+    size_t state_bytes = 0, reserve = 0, scratch_bytes = 0;
+    void *h_in = nullptr, *h_out = nullptr;   // pinned
+    double stats[GNSS_NSTATS] = {};
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    gnss_status status = GNSS_OK;
+    gnss_ctx *ctx = nullptr;
+    void *dev = nullptr, *scratch = nullptr;
+    gnss_fields state{}, hist{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int steps_issued = 0;
+    int phase = 0;   // 0 queued, 1 stepping, 2 copying out, 3 ended
+};
+
+}  // namespace
+
+// Pinned host buffers, reused across requests (page-locking is slow, so a
+// steady stream of requests allocates none).
+struct PinnedPool {
+    std::mutex mu;
+    std::multimap<size_t, void *> free_;
+    std::vector<void *> all;
+    void *get(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            auto it = free_.lower_bound(bytes);
+            if (it != free_.end() && it->first <= 2 * bytes) {
+                void *p = it->second;
+                free_.erase(it);
+                return p;
+            }
+        }
+        void *p = nullptr;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        all.push_back(p);
+        sizes[p] = bytes;
+        return p;
+    }
+    void put(void *p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lk(mu);
+        free_.emplace(sizes[p], p);
+    }
+    ~PinnedPool() {
+        for (void *p : all) cudaFreeHost(p);
+    }
+    std::map<void *, size_t> sizes;
+};
+
+struct gnss_server {
+    gnss_server_config cfg{};
+    PinnedPool pinned;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request *> pending;
+    std::vector<Request *> active;            // scheduler thread only (sizes read under mu)
+    std::map<long long, Request *> reqs;      // every request not yet fetched
+    std::vector<gnss_ctx *> retired;          // contexts of ended requests, destroyed with the server
+    long long next_id = 1;
+    bool stop = false;
+    gnss_server_report rep{};
+    Clock::time_point t0;
+    std::thread th;
+};
+
+static double now_s(const gnss_server *s) {
+    return std::chrono::duration<double>(Clock::now() - s->t0).count();
+}
+
+static void req_release_device(gnss_server *s, Request *r) {
+    if (r->gexec) {
+        cudaGraphExecDestroy(r->gexec);
+        r->gexec = nullptr;
+    }
+    if (r->dev) cudaFreeAsync(r->dev, r->stream);
+    if (r->scratch) cudaFreeAsync(r->scratch, r->stream);
+    r->dev = r->scratch = nullptr;
+    if (r->ev) cudaEventDestroy(r->ev);
+    if (r->stream) cudaStreamDestroy(r->stream);   // returns at once; pending frees still run
+    r->ev = nullptr;
+    r->stream = nullptr;
+    if (r->ctx) s->retired.push_back(r->ctx);
+    r->ctx = nullptr;
+}
+
+// Upload, dealias and the first step.  Runs on the scheduler thread.
+static gnss_status req_start(Request *r) {
+    const int nf = nfields_of(r->cfg);
+    const size_t fb = field_bytes_of(r->cfg);
+    if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess)
+        return GNSS_ERR_CUDA;
+    if (cudaMallocAsync(&r->dev, 2 * nf * fb, r->stream) != cudaSuccess ||
+        cudaMallocAsync(&r->scratch, r->scratch_bytes, r->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return GNSS_ERR_NOMEM;
+    }
+    r->state = fields_at(r->dev, fb, nf);
+    r->hist = fields_at(static_cast<char *>(r->dev) + nf * fb, fb, nf);
+    gnss_status st = gnss_attach_scratch(r->ctx, r->scratch, r->scratch_bytes);
+    if (st) return st;
+    if (cudaMemcpyAsync(r->dev, r->h_in, r->state_bytes, cudaMemcpyHostToDevice, r->stream) != cudaSuccess ||
+        cudaMemsetAsync(static_cast<char *>(r->dev) + nf * fb, 0, nf * fb, r->stream) != cudaSuccess)
+        return GNSS_ERR_CUDA;
+    void *f[5] = {r->state.u, r->state.v, r->state.w, r->state.s, r->state.c};
+    for (int q = 0; q < nf; ++q)
+        if ((st = gnss_dealias(r->ctx, f[q], r->stream))) return st;   // as gnss_run_host (main.cu:156)
+    if (r->n_steps > 0) {
+        if ((st = gnss_step(r->ctx, &r->state, &r->hist, 1, r->stream))) return st;
+        r->steps_issued = 1;
+    }
+    if (cudaEventRecord(r->ev, r->stream) != cudaSuccess) return GNSS_ERR_CUDA;
+    return GNSS_OK;
+}
+
+static gnss_status req_chunk(const gnss_server *s, Request *r) {
+    const int spl = std::max(1, s->cfg.steps_per_launch);
+    const int k = std::min(spl, r->n_steps - r->steps_issued);
+    gnss_status st = GNSS_OK;
+    if (k == spl && spl > 1) {
+        if (!r->gexec) {   // capture once per request, replay for every full chunk
+            if (cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return GNSS_ERR_CUDA;
+            for (int i = 0; i < k && !st; ++i) st = gnss_step(r->ctx, &r->state, &r->hist, 0, r->stream);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(r->stream, &g);
+            if (!st && ce != cudaSuccess) st = GNSS_ERR_CUDA;
+            if (!st && cudaGraphInstantiate(&r->gexec, g, 0) != cudaSuccess) st = GNSS_ERR_CUDA;
+            if (g) cudaGraphDestroy(g);
+            if (st) {
+                cudaGetLastError();
+                r->gexec = nullptr;
+                return st;
+            }
+        }
+        if (cudaGraphLaunch(r->gexec, r->stream) != cudaSuccess) return GNSS_ERR_CUDA;
+    } else {
+        for (int i = 0; i < k && !st; ++i) st = gnss_step(r->ctx, &r->state, &r->hist, 0, r->stream);
+        if (st) return st;
+    }
+    r->steps_issued += k;
+    return cudaEventRecord(r->ev, r->stream) == cudaSuccess ? GNSS_OK : GNSS_ERR_CUDA;
+}
+
+static gnss_status req_finish(Request *r) {
+    gnss_status st = gnss_stats(r->ctx, &r->state, r->stats, r->stream);   // the stream is idle here
+    if (st) return st;
+    if (cudaMemcpyAsync(r->h_out, r->dev, r->state_bytes, cudaMemcpyDeviceToHost, r->stream) != cudaSuccess ||
+        cudaEventRecord(r->ev, r->stream) != cudaSuccess)
+        return GNSS_ERR_CUDA;
+    return GNSS_OK;
+}
+
+static void server_loop(gnss_server *s) {
+    cudaSetDevice(s->cfg.device);
+    double busy_start = -1.0;
+    for (;;) {
+        std::vector<Request *> admit;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (s->active.empty() && (s->pending.empty() || s->stop)) {
+                if (busy_start >= 0) {
+                    s->rep.busy_seconds += now_s(s) - busy_start;
+                    busy_start = -1.0;
+                }
+                if (s->stop) break;
+                s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+                continue;
+            }
+            // admission in arrival order: the head waits until it fits
+            while (!s->stop && !s->pending.empty() &&
+                   (int)(s->active.size() + admit.size()) < std::max(1, s->cfg.max_active)) {
+                Request *r = s->pending.front();
+                if (s->rep.bytes_reserved + r->reserve > s->cfg.budget_bytes) {
+                    if (s->active.empty() && admit.empty()) {   // can never fit
+                        s->pending.pop_front();
+                        r->status = GNSS_ERR_NOMEM;
+                        r->phase = 3;
+                        r->t_done = now_s(s);
+                        s->rep.failed++;
+                        s->cv_done.notify_all();
+                        continue;
+                    }
+                    break;
+                }
+                s->pending.pop_front();
+                s->rep.bytes_reserved += r->reserve;
+                s->rep.bytes_reserved_max = std::max(s->rep.bytes_reserved_max, s->rep.bytes_reserved);
+                s->rep.admitted++;
+                admit.push_back(r);
+            }
+        }
+        bool progress = !admit.empty();
+        for (Request *r : admit) {
+            r->t_admit = now_s(s);
+            r->phase = 1;
+            r->status = req_start(r);
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->active.push_back(r);
+            s->rep.active_max = std::max(s->rep.active_max, (int)s->active.size());
+        }
+        if (!s->active.empty() && busy_start < 0) busy_start = now_s(s);
+        for (size_t i = 0; i < s->active.size();) {
+            Request *r = s->active[i];
+            if (r->status == GNSS_OK && r->ev) {
+                const cudaError_t q = cudaEventQuery(r->ev);
+                if (q == cudaErrorNotReady) {
+                    ++i;
+                    continue;
+                }
+                if (q != cudaSuccess) r->status = GNSS_ERR_CUDA;
+            }
+            progress = true;
+            if (r->status == GNSS_OK && r->phase == 1) {
+                if (r->steps_issued < r->n_steps) {
+                    r->status = req_chunk(s, r);
+                } else {   // every step has run: statistics and copy-out
+                    r->status = req_finish(r);
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    if (r->status == GNSS_OK) r->phase = 2;
+                }
+            }
+            ++i;
+        }
+        // requests whose copy-out completed (phase 2), or that failed, end here
+        for (size_t i = 0; i < s->active.size();) {
+            Request *r = s->active[i];
+            const bool done = r->status != GNSS_OK || (r->phase == 2 && cudaEventQuery(r->ev) == cudaSuccess);
+            if (!done) {
+                ++i;
+                continue;
+            }
+            progress = true;
+            req_release_device(s, r);
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->t_done = now_s(s);
+            r->phase = 3;
+            s->rep.bytes_reserved -= r->reserve;
+            if (r->status == GNSS_OK) {
+                s->rep.completed++;
+                s->rep.point_steps += (double)r->cfg.nx * r->cfg.ny * r->cfg.nz * r->n_steps;
+            } else {
+                s->rep.failed++;
+            }
+            s->active.erase(s->active.begin() + (long)i);
+            s->cv_done.notify_all();
+        }
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+gnss_status gnss_server_create(const gnss_server_config *cfg, gnss_server **out) {
+    if (!cfg || !out || cfg->max_active < 1 || cfg->steps_per_launch < 1) return GNSS_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) {
+        cudaGetLastError();
+        return GNSS_ERR_CUDA;
+    }
+    gnss_server *s = new gnss_server;
+    s->cfg = *cfg;
+    s->t0 = Clock::now();
+    s->th = std::thread(server_loop, s);
+    *out = s;
+    return GNSS_OK;
+}
+
+gnss_status gnss_server_destroy(gnss_server *s) {
+    if (!s) return GNSS_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        for (Request *r : s->pending) {   // dropped
+            r->status = GNSS_ERR_INVALID;
+            r->phase = 3;
+        }
+        s->pending.clear();
+    }
+    s->cv_work.notify_all();
+    s->th.join();
+    cudaSetDevice(s->cfg.device);
+    cudaDeviceSynchronize();
+    for (gnss_ctx *c : s->retired) gnss_destroy(c);
+    for (auto &kv : s->reqs) {
+        Request *r = kv.second;
+        if (r->ctx) gnss_destroy(r->ctx);
+        delete r;   // pinned buffers go with the pool
+    }
+    delete s;
+    return GNSS_OK;
+}
+
+gnss_status gnss_server_submit(gnss_server *s, const gnss_config *cfg, const void *host_state, int n_steps,
+                               long long *id) {
+    if (!s || !cfg || !host_state || n_steps < 0) return GNSS_ERR_INVALID;
+    if (cfg->device != s->cfg.device) return GNSS_ERR_INVALID;
+    const double t_entry = now_s(s);
+    Request *r = new Request;
+    r->cfg = *cfg;
+    r->n_steps = n_steps;
+    gnss_status st = gnss_create(cfg, &r->ctx);
+    if (st) {
+        delete r;
+        return st;
+    }
+    const int nf = nfields_of(*cfg);
+    const size_t fb = field_bytes_of(*cfg);
+    r->state_bytes = nf * fb;
+    r->scratch_bytes = round256(gnss_scratch_bytes(r->ctx));
+    r->reserve = 2 * nf * fb + r->scratch_bytes + gnss_workspace_bytes(r->ctx);
+    r->h_in = s->pinned.get(r->state_bytes);
+    r->h_out = s->pinned.get(r->state_bytes);
+    if (!r->h_in || !r->h_out) {
+        s->pinned.put(r->h_in);
+        s->pinned.put(r->h_out);
+        gnss_destroy(r->ctx);
+        delete r;
+        return GNSS_ERR_NOMEM;
+    }
+    std::memcpy(r->h_in, host_state, r->state_bytes);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            s->pinned.put(r->h_in);
+            s->pinned.put(r->h_out);
+            gnss_destroy(r->ctx);
+            delete r;
+            return GNSS_ERR_INVALID;
+        }
+        r->id = s->next_id++;
+        r->t_submit = t_entry;   // latency counts the submission's own copy
+        s->reqs[r->id] = r;
+        s->pending.push_back(r);
+        s->rep.submitted++;
+    }
+    s->cv_work.notify_one();
+    if (id) *id = r->id;
+    return GNSS_OK;
+}
+
+gnss_status gnss_server_wait(gnss_server *s, long long id, double timeout_s) {
+    if (!s) return GNSS_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return GNSS_ERR_INVALID;
+    Request *r = it->second;
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return r->phase == 3; });
+    return ok ? GNSS_OK : GNSS_ERR_TIMEOUT;
+}
+
+gnss_status gnss_server_result(gnss_server *s, long long id, void *host_state_out, double *stats, double *times) {
+    if (!s) return GNSS_ERR_INVALID;
+    Request *r = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(id);
+        if (it == s->reqs.end() || it->second->phase != 3) return GNSS_ERR_INVALID;
+        r = it->second;
+        s->reqs.erase(it);
+    }
+    const gnss_status st = r->status;
+    if (st == GNSS_OK) {
+        if (host_state_out) std::memcpy(host_state_out, r->h_out, r->state_bytes);
+        if (stats) std::memcpy(stats, r->stats, sizeof r->stats);
+    }
+    if (times) {
+        times[0] = r->t_submit;
+        times[1] = r->t_admit;
+        times[2] = r->t_done;
+    }
+    if (r->ctx) gnss_destroy(r->ctx);   // never admitted
+    s->pinned.put(r->h_in);
+    s->pinned.put(r->h_out);
+    delete r;
+    return st;
+}
+
+gnss_status gnss_server_report_get(gnss_server *s, gnss_server_report *out) {
+    if (!s || !out) return GNSS_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->rep;
+    return GNSS_OK;
+}

@@ -25,6 +25,7 @@ struct gnss_ctx {
     void *tw[3] = {nullptr, nullptr, nullptr};   // twiddle tables for nx, ny, nz
     void *scratch = nullptr;                      // nscratch fields
     int nscratch = 0;
+    bool scratch_ext = false;                     // scratch attached by the caller (not owned)
     double *stat_part = nullptr;                  // STAT_BLOCKS x STAT_SUMS
     double *stat_dev = nullptr;                   // STAT_SUMS
     double *stat_host = nullptr;                  // pinned STAT_SUMS
@@ -321,6 +322,8 @@ template <typename T> static V2<T> *fld(void *base, size_t nspec, int i) {
 
 static gnss_status ensure_scratch(gnss_ctx *c, int nfields) {
     if (c->nscratch >= nfields) return GNSS_OK;
+    if (c->scratch_ext)
+        return fail(c, GNSS_ERR_NOMEM, "attached scratch holds %d fields, %d needed", c->nscratch, nfields);
     if (c->scratch) {
         cudaFree(c->scratch);
         c->owned_bytes -= (size_t)c->nscratch * c->nspec * c->elem;
@@ -755,6 +758,34 @@ gnss_status gnss_profile_read(gnss_ctx *c, double *ms, long long *launches) {
 size_t gnss_field_bytes(const gnss_ctx *ctx) { return ctx ? ctx->nspec * ctx->elem : 0; }
 size_t gnss_workspace_bytes(const gnss_ctx *ctx) { return ctx ? ctx->owned_bytes : 0; }
 
+// scratch fields any operation of this context can ask for (the step's, or one field for the transforms)
+static int scratch_fields_max(const gnss_ctx *c) {
+    const size_t need = step_scratch_elems(c);
+    const int nf = (int)((need + c->nspec - 1) / c->nspec);
+    return nf > 1 ? nf : 1;
+}
+
+size_t gnss_scratch_bytes(const gnss_ctx *c) {
+    return c ? (size_t)scratch_fields_max(c) * c->nspec * c->elem : 0;
+}
+
+gnss_status gnss_attach_scratch(gnss_ctx *c, void *ptr, size_t bytes) {
+    if (!c) return GNSS_ERR_INVALID;
+    if (!ptr || (reinterpret_cast<uintptr_t>(ptr) % 256) != 0)
+        return fail(c, GNSS_ERR_INVALID, "scratch must be a 256-byte aligned device pointer");
+    if (bytes < gnss_scratch_bytes(c))
+        return fail(c, GNSS_ERR_INVALID, "scratch of %zu bytes, %zu needed", bytes, gnss_scratch_bytes(c));
+    CK(c, cudaSetDevice(c->cfg.device));
+    if (c->scratch && !c->scratch_ext) {
+        cudaFree(c->scratch);
+        c->owned_bytes -= (size_t)c->nscratch * c->nspec * c->elem;
+    }
+    c->scratch = ptr;
+    c->scratch_ext = true;
+    c->nscratch = (int)(bytes / (c->nspec * c->elem));
+    return GNSS_OK;
+}
+
 template <typename T> static void *make_twiddles(int n, gnss_ctx *c) {
     std::vector<V2<T>> h(n);
     const long double twopi = 6.283185307179586476925286766559L;
@@ -952,7 +983,7 @@ gnss_status gnss_destroy(gnss_ctx *c) {
     if (!c) return GNSS_ERR_INVALID;
     cudaSetDevice(c->cfg.device);
     for (int a = 0; a < 3; ++a) if (c->tw[a]) cudaFree(c->tw[a]);
-    if (c->scratch) cudaFree(c->scratch);
+    if (c->scratch && !c->scratch_ext) cudaFree(c->scratch);
     if (c->stat_part) cudaFree(c->stat_part);
     if (c->stat_dev) cudaFree(c->stat_dev);
     if (c->stat_host) cudaFreeHost(c->stat_host);

@@ -13,8 +13,8 @@
 // A line therefore crosses shared memory once per transform (instead of once
 // per radix-8 stage), the C2R packing is done while loading the registers,
 // and the twiddles of step A are products of four table powers.  Physical
-// values are exchanged between warps through one bank of lines; two block
-// barriers per line pair.
+// values are exchanged between warps through one bank of lines; the whole
+// block forms the products into the scratch lines of the forward warps.
 #pragma once
 #include "kernels.cuh"
 
@@ -221,48 +221,42 @@ __device__ __forceinline__ void zr_pack(int lane, V2<T> *x, const ZRecipe rc, co
     }
 }
 
-// Product f of the physical quantities at elements lane + 32 m (the input
-// layout of zr_fft).  Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3, 6 sx, 7 sy,
-// 8 sz, [9 cx, 10 cy, 11 cz], [12 c, 13 lap s]; products as zphys_products.
+// Pointwise products of one line pair by the whole block: point n of product
+// f goes to element pidx(n) of line f of `out` (the scratch lines of the
+// forward warps, stride SCR).  Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3,
+// 6 sx, 7 sy, 8 sz, [9 cx, 10 cy, 11 cz], [12 c, 13 lap s]; products as
+// zphys_products: (w x u) (crossProductKernel_mgpu, solver.cu:139-164),
+// u . grad s (dotKernel_mgpu, solver.cu:342-356) and the colloid term
+// (colloidAdvectionKernel_mgpu, solver.cu:374-388).
 template <typename T, int N, int NPH>
-__device__ __forceinline__ void zr_products(int f, int lane, V2<T> *x, const V2<T> *phys, T alpha) {
+__device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alpha) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
-    constexpr int E = Z::E, PL = Z::PL;
+    constexpr int PL = Z::PL, SCR = Z::SCR;
     constexpr bool has_c = NPH >= 12, has_al = NPH >= 14;
-#pragma unroll
-    for (int m = 0; m < E; ++m) {
-        const V *p = phys + Z::pidx(lane + 32 * m);
-        auto q = [&](int i) -> V { return p[i * PL]; };
-        V r;
-        if (f == 0) {          // (w x u)_x  (crossProductKernel_mgpu, solver.cu:139-164)
-            const V o2 = q(4), w = q(2), o3 = q(5), v = q(1);
-            r = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
-        } else if (f == 1) {   // (w x u)_y
-            const V o1 = q(3), w = q(2), o3 = q(5), u = q(0);
-            r = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
-        } else if (f == 2) {   // (w x u)_z
-            const V o1 = q(3), v = q(1), o2 = q(4), u = q(0);
-            r = V{o1.x * v.x - o2.x * u.x, o1.y * v.y - o2.y * u.y};
-        } else if (f == 3) {   // u . grad s  (dotKernel_mgpu, solver.cu:342-356)
-            const V u = q(0), v = q(1), w = q(2), sx = q(6), sy = q(7), sz = q(8);
-            r = V{u.x * sx.x + v.x * sy.x + w.x * sz.x, u.y * sx.y + v.y * sy.y + w.y * sz.y};
-        } else {               // colloid term (colloidAdvectionKernel_mgpu, solver.cu:374-388)
-            r = V{T(0), T(0)};
-            if constexpr (has_c) {
-                const V u = q(0), v = q(1), w = q(2), cx = q(9), cy = q(10), cz = q(11);
-                const V adv = V{u.x * cx.x + v.x * cy.x + w.x * cz.x, u.y * cx.y + v.y * cy.y + w.y * cz.y};
-                if constexpr (has_al) {
-                    const V sx = q(6), sy = q(7), sz = q(8), cc = q(12), ls = q(13);
-                    const V dr = V{ls.x * cc.x + cx.x * sx.x + cy.x * sy.x + cz.x * sz.x,
-                                   ls.y * cc.y + cx.y * sx.y + cy.y * sy.y + cz.y * sz.y};
-                    r = V{alpha * dr.x + adv.x, alpha * dr.y + adv.y};
-                } else {
-                    r = adv;
-                }
+    for (int n = threadIdx.x; n < N; n += blockDim.x) {
+        const int pn = Z::pidx(n);
+        const V *p = phys + pn;
+        const V u = p[0 * PL], v = p[1 * PL], w = p[2 * PL];
+        const V o1 = p[3 * PL], o2 = p[4 * PL], o3 = p[5 * PL];
+        const V sx = p[6 * PL], sy = p[7 * PL], sz = p[8 * PL];
+        V *o = out + pn;
+        o[0 * SCR] = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
+        o[1 * SCR] = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
+        o[2 * SCR] = V{o1.x * v.x - o2.x * u.x, o1.y * v.y - o2.y * u.y};
+        o[3 * SCR] = V{u.x * sx.x + v.x * sy.x + w.x * sz.x, u.y * sx.y + v.y * sy.y + w.y * sz.y};
+        if constexpr (has_c) {
+            const V cx = p[9 * PL], cy = p[10 * PL], cz = p[11 * PL];
+            const V adv = V{u.x * cx.x + v.x * cy.x + w.x * cz.x, u.y * cx.y + v.y * cy.y + w.y * cz.y};
+            if constexpr (has_al) {
+                const V cc = p[12 * PL], ls = p[13 * PL];
+                const V dr = V{ls.x * cc.x + cx.x * sx.x + cy.x * sy.x + cz.x * sz.x,
+                               ls.y * cc.y + cx.y * sx.y + cy.y * sy.y + cz.y * sz.y};
+                o[4 * SCR] = V{alpha * dr.x + adv.x, alpha * dr.y + adv.y};
+            } else {
+                o[4 * SCR] = adv;
             }
         }
-        x[m] = r;
     }
 }
 
@@ -323,8 +317,12 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
 #pragma unroll
         for (int q = 0; q < E; ++q) myphys[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
         __syncthreads();   // every physical quantity on chip
+        zr_products<T, N, NPH>(phys, scr_all, alpha);
+        __syncthreads();   // products in the scratch lines of warps 0 .. nout-1
         if (warp < nout) {   // z R2C of product `warp`, written over raw field `warp` of the pair
-            zr_products<T, N, NPH>(warp, lane, x, phys, alpha);
+#pragma unroll
+            for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
+            __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
 #pragma unroll
             for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = x[q];

@@ -96,6 +96,25 @@ _SIGS = {
     "gnss_set_option": [_VP, ctypes.c_int, ctypes.c_int],
     "gnss_get_option": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
+    "gnss_scratch_bytes": [_VP],
+    "gnss_attach_scratch": [_VP, _VP, ctypes.c_size_t],
+    "gnss_ensemble_create": [ctypes.POINTER(GnssConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "gnss_ensemble_destroy": [_VP],
+    "gnss_ensemble_size": [_VP],
+    "gnss_ensemble_member": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(GnssFields),
+                             ctypes.POINTER(GnssFields)],
+    "gnss_ensemble_upload": [_VP, ctypes.c_int, _VP, _VP],
+    "gnss_ensemble_download": [_VP, ctypes.c_int, _VP, _VP],
+    "gnss_ensemble_step": [_VP, ctypes.c_int, _VP],
+    "gnss_ensemble_launches_per_step": [_VP],
+    "gnss_ensemble_autotune": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
+    "gnss_server_create": [_VP, ctypes.POINTER(ctypes.c_void_p)],
+    "gnss_server_destroy": [_VP],
+    "gnss_server_submit": [_VP, ctypes.POINTER(GnssConfig), _VP, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)],
+    "gnss_server_wait": [_VP, ctypes.c_longlong, ctypes.c_double],
+    "gnss_server_result": [_VP, ctypes.c_longlong, _VP, ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_double)],
+    "gnss_server_report_get": [_VP, _VP],
 }
 _RESTYPES = {
     "gnss_field_bytes": ctypes.c_size_t,
@@ -103,6 +122,9 @@ _RESTYPES = {
     "gnss_status_string": ctypes.c_char_p,
     "gnss_last_error": ctypes.c_char_p,
     "gnss_launch_count": ctypes.c_longlong,
+    "gnss_scratch_bytes": ctypes.c_size_t,
+    "gnss_ensemble_size": ctypes.c_int,
+    "gnss_ensemble_launches_per_step": ctypes.c_longlong,
 }
 STAGE_NAMES = ("x_inverse", "y_inverse", "z_physical", "y_forward", "x_forward", "spectral_update")
 
@@ -164,27 +186,42 @@ def _fields(fs: Sequence | None) -> GnssFields | None:
     return GnssFields(*p[:5])
 
 
+def make_config(n: int | None = None, *, nx: int | None = None, ny: int | None = None, nz: int | None = None,
+                lx: float = 2 * math.pi, ly: float = 2 * math.pi, lz: float = 2 * math.pi, re: float = 1000.0,
+                sc: float = 0.7, sc_c: float = 0.7, alpha: float = 0.0, dt: float = 1e-3,
+                alias_filter: float = 2.0 / 3.0, nu_stats: float | None = None, n_scalars: int = 1,
+                scheme: int = GNSS_SCHEME_CNAB2, precision: int = GNSS_FP64, device: int = 0) -> GnssConfig:
+    """A gnss_config with the reference's defaults (dnsparams.h: LX = LY = LZ = 2 pi, nu = H/Re, H = 1)."""
+    nx, ny, nz = nx or n, ny or n, nz or n
+    if nu_stats is None:
+        nu_stats = 1.0 / re   # the reference's nu = H/Re with H = 1 (dnsparams.h:30)
+    return GnssConfig(nx, ny, nz, lx, ly, lz, re, sc, sc_c, alpha, dt, alias_filter, nu_stats,
+                      n_scalars, scheme, precision, device)
+
+
 class Context:
     """One grid configuration on one device (replaces plan1dFFT/plan2dFFT and
     the global state of the reference, fftfuncs.cu:133-231, declare.h)."""
 
-    def __init__(self, n: int | None = None, *, nx: int | None = None, ny: int | None = None,
-                 nz: int | None = None, lx: float = 2 * math.pi, ly: float = 2 * math.pi,
-                 lz: float = 2 * math.pi, re: float = 1000.0, sc: float = 0.7, sc_c: float = 0.7,
-                 alpha: float = 0.0, dt: float = 1e-3, alias_filter: float = 2.0 / 3.0,
-                 nu_stats: float | None = None, n_scalars: int = 1, scheme: int = GNSS_SCHEME_CNAB2,
-                 precision: int = GNSS_FP64, device: int = 0):
+    def __init__(self, n: int | None = None, **kw):
         self.lib = load_library()
-        nx, ny, nz = nx or n, ny or n, nz or n
-        if nu_stats is None:
-            nu_stats = 1.0 / re   # the reference's nu = H/Re with H = 1 (dnsparams.h:30)
-        self.cfg = GnssConfig(nx, ny, nz, lx, ly, lz, re, sc, sc_c, alpha, dt, alias_filter, nu_stats,
-                              n_scalars, scheme, precision, device)
+        self.cfg = make_config(n, **kw)
+        self._owned = True
         h = ctypes.c_void_p()
         st = self.lib.gnss_create(ctypes.byref(self.cfg), ctypes.byref(h))
         if st != GNSS_OK:
             raise GnssError(st, "gnss_create", self.lib.gnss_status_string(st).decode())
         self._h = h
+
+    @classmethod
+    def _borrow(cls, handle, cfg: GnssConfig) -> "Context":
+        """A view of a context owned elsewhere (an ensemble member); close() does not destroy it."""
+        c = cls.__new__(cls)
+        c.lib = load_library()
+        c.cfg = cfg
+        c._owned = False
+        c._h = handle
+        return c
 
     # -- bookkeeping -------------------------------------------------------
     @property
@@ -222,7 +259,8 @@ class Context:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            self.lib.gnss_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self.lib.gnss_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -464,3 +502,159 @@ def pack_state(fields: Sequence[np.ndarray], out: np.ndarray | None = None) -> n
     for q, f in enumerate(fields):
         out[q * n:(q + 1) * n] = f.ravel()
     return out
+
+
+# ---------------------------------------------------------------------- batching
+class Ensemble:
+    """Many independent jets stepped together (gnss_ensemble_*): every member's
+    steps after the first are one CUDA graph launch.  configs: GnssConfig
+    values (make_config); all on one device."""
+
+    def __init__(self, configs: Sequence[GnssConfig], n_branches: int = 4):
+        self.lib = load_library()
+        self.configs = list(configs)
+        arr = (GnssConfig * len(self.configs))(*self.configs)
+        h = ctypes.c_void_p()
+        st = self.lib.gnss_ensemble_create(arr, len(self.configs), int(n_branches), ctypes.byref(h))
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_ensemble_create", self.lib.gnss_status_string(st).decode())
+        self._h = h
+
+    def __len__(self) -> int:
+        return int(self.lib.gnss_ensemble_size(self._h))
+
+    def member(self, i: int):
+        """(Context view, state GnssFields, history GnssFields) of member i."""
+        ch = ctypes.c_void_p()
+        sf, hf = GnssFields(), GnssFields()
+        self._ck(self.lib.gnss_ensemble_member(self._h, i, ctypes.byref(ch), ctypes.byref(sf), ctypes.byref(hf)),
+                 "gnss_ensemble_member")
+        return Context._borrow(ch, self.configs[i]), sf, hf
+
+    def upload(self, i: int, host_state, stream=None) -> None:
+        self._ck(self.lib.gnss_ensemble_upload(self._h, i, _host_ptr(host_state), _stream(stream)),
+                 "gnss_ensemble_upload")
+
+    def download(self, i: int, host_state, stream=None) -> None:
+        self._ck(self.lib.gnss_ensemble_download(self._h, i, _host_ptr(host_state), _stream(stream)),
+                 "gnss_ensemble_download")
+
+    def step(self, n_steps: int, stream=None) -> None:
+        self._ck(self.lib.gnss_ensemble_step(self._h, int(n_steps), _stream(stream)), "gnss_ensemble_step")
+
+    def launches_per_step(self) -> int:
+        return int(self.lib.gnss_ensemble_launches_per_step(self._h))
+
+    def autotune(self, steps: int = 3) -> list:
+        ch = (ctypes.c_int * len(self.configs))()
+        self._ck(self.lib.gnss_ensemble_autotune(self._h, int(steps), ch), "gnss_ensemble_autotune")
+        return list(ch)
+
+    def stats(self, i: int, stream=None) -> dict:
+        ctx, sf, _ = self.member(i)
+        out = (ctypes.c_double * GNSS_NSTATS)()
+        self._ck(self.lib.gnss_stats(ctx._h, ctypes.byref(sf), out, _stream(stream)), "gnss_stats")
+        return {k: float(out[j]) for j, k in enumerate(STAT_NAMES)}
+
+    def points(self) -> float:
+        return float(sum(c.nx * c.ny * c.nz for c in self.configs))
+
+    def _ck(self, st: int, what: str) -> None:
+        if st != GNSS_OK:
+            raise GnssError(st, what, self.lib.gnss_status_string(st).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.gnss_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int),
+                ("steps_per_launch", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class ServerReport(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("admitted", ctypes.c_longlong),
+                ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("bytes_reserved", ctypes.c_size_t), ("bytes_reserved_max", ctypes.c_size_t),
+                ("active_max", ctypes.c_int), ("point_steps", ctypes.c_double),
+                ("busy_seconds", ctypes.c_double)]
+
+
+class Server:
+    """Continuous-batching request loop (gnss_server_*): jets are admitted in
+    arrival order under a device-memory budget, stay resident while they run,
+    and advance concurrently on their own streams."""
+
+    def __init__(self, budget_bytes: int, max_active: int = 32, steps_per_launch: int = 20, device: int = 0):
+        self.lib = load_library()
+        cfg = ServerConfig(int(budget_bytes), int(max_active), int(steps_per_launch), int(device))
+        h = ctypes.c_void_p()
+        st = self.lib.gnss_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_server_create", self.lib.gnss_status_string(st).decode())
+        self._h = h
+        self._shapes = {}
+
+    def submit(self, cfg: GnssConfig, host_state: np.ndarray, n_steps: int) -> int:
+        """Queue a jet run; host_state: packed fields (pack_state), copied at submission."""
+        a = np.ascontiguousarray(host_state)
+        rid = ctypes.c_longlong()
+        st = self.lib.gnss_server_submit(self._h, ctypes.byref(cfg), a.ctypes.data, int(n_steps), ctypes.byref(rid))
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_server_submit", self.lib.gnss_status_string(st).decode())
+        self._shapes[rid.value] = (a.shape, a.dtype)
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = 600.0) -> None:
+        st = self.lib.gnss_server_wait(self._h, int(rid), float(timeout))
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_server_wait", self.lib.gnss_status_string(st).decode())
+
+    def result(self, rid: int):
+        """(final packed state, statistics dict, (submitted, admitted, finished) seconds)."""
+        shape, dtype = self._shapes.pop(rid)
+        out = np.empty(shape, dtype=dtype)
+        stats = (ctypes.c_double * GNSS_NSTATS)()
+        times = (ctypes.c_double * 3)()
+        st = self.lib.gnss_server_result(self._h, int(rid), out.ctypes.data, stats, times)
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_server_result", self.lib.gnss_status_string(st).decode())
+        return out, {k: float(stats[j]) for j, k in enumerate(STAT_NAMES)}, tuple(times)
+
+    def report(self) -> dict:
+        r = ServerReport()
+        st = self.lib.gnss_server_report_get(self._h, ctypes.byref(r))
+        if st != GNSS_OK:
+            raise GnssError(st, "gnss_server_report_get")
+        return {k: getattr(r, k) for k, _ in ServerReport._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.gnss_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -204,6 +204,94 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 gnss_status gnss_set_option(gnss_ctx *ctx, int key, int value);
 gnss_status gnss_get_option(const gnss_ctx *ctx, int key, int *value);
 
+/* Scratch of a context.  gnss_scratch_bytes: the device bytes every
+ * operation of the context can ask for (the fused step's intermediates, or
+ * one field for the transforms).  gnss_attach_scratch: use caller memory
+ * (256-byte aligned, at least gnss_scratch_bytes) instead of the context's
+ * own; the context frees its own scratch and never frees the attached one.
+ * Contexts whose work is ordered on one stream may share one buffer.  No
+ * counterpart in the reference (fft.temp / fft.wspace, allocate.cu:9-225). */
+size_t gnss_scratch_bytes(const gnss_ctx *ctx);
+gnss_status gnss_attach_scratch(gnss_ctx *ctx, void *scratch, size_t bytes);
+
+/* ---------------------------------------------------------------- batching
+ * An ensemble of independent jets (uneven grids, Reynolds and Schmidt
+ * numbers) stepped together.  The library owns every member's state and
+ * history; members are spread over n_branches streams (longest first, each to
+ * the least-loaded branch) and the members of one branch share one scratch
+ * buffer.  gnss_ensemble_step runs n_steps steps of every member: the first
+ * step of a run (Euler, for GNSS_SCHEME_CNAB2) is launched directly, and
+ * the rest as ONE CUDA graph launch that holds all members' steps in
+ * parallel branches (captured on first use for that step count, replayed
+ * afterwards).  A member's result is bit-identical to stepping it alone with
+ * gnss_step.  No counterpart in the reference (one jet per program). */
+typedef struct gnss_ensemble gnss_ensemble;
+gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n_members, int n_branches, gnss_ensemble **out);
+gnss_status gnss_ensemble_destroy(gnss_ensemble *e);
+int gnss_ensemble_size(const gnss_ensemble *e);
+/* Member i: its context (owned by the ensemble) and its device state and
+ * history (zeroed at creation; upload and dealias the state before the first
+ * step, e.g. with cudaMemcpy + gnss_dealias). */
+gnss_status gnss_ensemble_member(gnss_ensemble *e, int i, gnss_ctx **ctx, gnss_fields *state, gnss_fields *hist);
+/* Copy member i's state from / to packed host memory (3 + n_scalars fields
+ * back to back, pinned for asynchronous copies).  Upload also zeroes the
+ * member's history and dealiases the state (main.cu:156); upload every
+ * member before the first step.  Download synchronises the stream. */
+gnss_status gnss_ensemble_upload(gnss_ensemble *e, int i, const void *host_state, void *stream);
+gnss_status gnss_ensemble_download(gnss_ensemble *e, int i, void *host_state, void *stream);
+gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream);
+/* Kernels launched per step of the whole ensemble (for launch accounting). */
+long long gnss_ensemble_launches_per_step(const gnss_ensemble *e);
+/* Autotuner: for every member, time each kernel variant (GNSS_OPT_*) over
+ * `steps` steps on the member's own buffers (which are zeroed afterwards, so
+ * tune before uploading states) and keep the fastest.  Members of equal
+ * (grid, precision, scalars, scheme) share one measurement.  choices (may be
+ * NULL) receives the chosen GNSS_OPT_ZVARIANT value per member. */
+gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop with continuous batching.  Requests (a configuration, a
+ * packed host state of 3 + n_scalars spectral fields, a step count) are
+ * queued by gnss_server_submit from any host thread.  A scheduler thread
+ * admits them in arrival order as soon as an active slot and enough of the
+ * device-memory budget are free (state, history and scratch are reserved at
+ * admission and stay on the device until the request ends), uploads and
+ * dealiases the state, and advances every active request on its own stream
+ * in chunks of steps_per_launch steps (one CUDA graph launch per chunk), so
+ * the work of requests in flight overlaps on the device.  A finished request
+ * keeps its final state and statistics until gnss_server_result.  A
+ * request's result is bit-identical to gnss_run_host on the same input,
+ * whatever else is in flight.  Times are seconds since the server started. */
+typedef struct gnss_server gnss_server;
+typedef struct gnss_server_config {
+    size_t budget_bytes;     /* device memory the server may reserve for requests  */
+    int max_active;          /* requests in flight at most                          */
+    int steps_per_launch;    /* steps per graph launch of one request               */
+    int device;              /* CUDA device ordinal                                 */
+} gnss_server_config;
+typedef struct gnss_server_report {
+    long long submitted, admitted, completed, failed;
+    size_t bytes_reserved;       /* now                                             */
+    size_t bytes_reserved_max;   /* the most reserved at any time                   */
+    int active_max;              /* the most requests in flight at any time         */
+    double point_steps;          /* sum over completed requests of nx*ny*nz*steps   */
+    double busy_seconds;         /* wall time with at least one request in flight    */
+} gnss_server_report;
+gnss_status gnss_server_create(const gnss_server_config *cfg, gnss_server **out);
+/* Stops the scheduler after the requests in flight end; pending requests are
+ * dropped. */
+gnss_status gnss_server_destroy(gnss_server *srv);
+gnss_status gnss_server_submit(gnss_server *srv, const gnss_config *cfg, const void *host_state, int n_steps,
+                               long long *id);
+/* Blocks until request id has ended (GNSS_ERR_TIMEOUT after timeout_s). */
+gnss_status gnss_server_wait(gnss_server *srv, long long id, double timeout_s);
+/* Final state (packed like the input; may be NULL), statistics after the last
+ * step (GNSS_NSTATS doubles; may be NULL) and times {submitted, admitted,
+ * finished} (may be NULL) of an ended request, which is then forgotten.
+ * Returns the request's own status (GNSS_ERR_* if it failed). */
+gnss_status gnss_server_result(gnss_server *srv, long long id, void *host_state_out, double *stats, double *times);
+gnss_status gnss_server_report_get(gnss_server *srv, gnss_server_report *out);
+
 /* Forward transform that allocates nothing.  No counterpart in the
  * reference.  For callers that may not allocate device memory: code running
  * under a memory manager that owns the whole device (a framework's caching
