@@ -267,7 +267,9 @@ def run_ensemble(G, torch, dev, steps, branches=8) -> dict:
                         "FP32, dt 1e-3, cnab2",
             "graph": f"{chunk} steps of all 32 members per CUDA graph launch, {branches} branches",
             "gpu_launches_per_step": lps, "autotune_s": round(t_tune, 2),
-            "autotune_choices": {str(n): int(choices[ENSEMBLE_SIZES.index(n)]) for n in sorted(set(ENSEMBLE_SIZES))},
+            "autotune_choices": {str(n): {"z": ("auto", "register", "staged")[choices[ENSEMBLE_SIZES.index(n)] & 3],
+                                          "pass": ("auto", "register", "staged")[choices[ENSEMBLE_SIZES.index(n)] >> 2]}
+                                 for n in sorted(set(ENSEMBLE_SIZES))},
             "clocks": clk.summary()}
 
 

@@ -282,15 +282,18 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     gnss_status st = GNSS_OK;
-    const int variants[2] = {GNSS_ZVARIANT_AUTO, GNSS_ZVARIANT_STAGED};
+    const int variants[2] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED};
     for (Member &mb : e->m) {
         const Key k{mb.cfg.nx, mb.cfg.ny, mb.cfg.nz, mb.cfg.precision, mb.cfg.n_scalars, mb.cfg.scheme};
         if (best.count(k)) continue;
         const cudaStream_t bs = e->streams[mb.branch];
         float tbest = 0.f;
-        int vbest = GNSS_ZVARIANT_AUTO;
-        for (int v : variants) {
-            if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v))) break;
+        int vbest = 0;
+        for (int combo = 0; combo < 4; ++combo) {
+            const int v = variants[combo & 1] + 4 * variants[combo >> 1];   // z variant + 4 * pass variant
+            if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, variants[combo & 1])) ||
+                (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, variants[combo >> 1])))
+                break;
             if ((st = gnss_step(mb.ctx, &mb.state, &mb.hist, 1, bs))) break;   // warm-up
             cudaEventRecord(t0, bs);
             for (int i = 0; i < steps && !st; ++i) st = gnss_step(mb.ctx, &mb.state, &mb.hist, 0, bs);
@@ -299,7 +302,7 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
             cudaEventSynchronize(t1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, t0, t1);
-            if (v == variants[0] || ms < tbest) {
+            if (combo == 0 || ms < tbest) {
                 tbest = ms;
                 vbest = v;
             }
@@ -313,7 +316,9 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     for (size_t i = 0; i < e->m.size(); ++i) {
         Member &mb = e->m[i];
         const int v = best[Key{mb.cfg.nx, mb.cfg.ny, mb.cfg.nz, mb.cfg.precision, mb.cfg.n_scalars, mb.cfg.scheme}];
-        if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v))) return st;
+        if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v & 3)) ||
+            (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, v >> 2)))
+            return st;
         if (choices) choices[i] = v;
         const size_t fb = field_bytes_of(mb.cfg);
         if (cudaMemset(mb.buf, 0, 2 * nfields_of(mb.cfg) * fb) != cudaSuccess) return GNSS_ERR_CUDA;

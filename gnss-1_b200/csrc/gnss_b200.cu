@@ -13,6 +13,8 @@
 #include "gnss_b200.h"
 #include "kernels.cuh"
 #include "zreg.cuh"
+#include "passreg.cuh"
+#include "diag.cuh"
 
 using namespace gnss;
 
@@ -29,6 +31,9 @@ struct gnss_ctx {
     double *stat_part = nullptr;                  // STAT_BLOCKS x STAT_SUMS
     double *stat_dev = nullptr;                   // STAT_SUMS
     double *stat_host = nullptr;                  // pinned STAT_SUMS
+    double *turb_part = nullptr;                  // STAT_BLOCKS x TURB_SUMS (gnss_turb_stats)
+    double *turb_dev = nullptr;                   // TURB_SUMS + 1 sums, then 5 * ny profile values
+    double *turb_host = nullptr;                  // pinned copy of turb_dev
     void *res = nullptr;                          // resident state + history for gnss_run_host (2 * nf fields)
     size_t owned_bytes = 0;
     // fused step layout (set_recipes): x-inverse outputs P, y-inverse outputs
@@ -39,7 +44,8 @@ struct gnss_ctx {
     KeepMap kx_keep{}, ky_keep{};
     int nkz = 0, ncp = 0;
     size_t p_elems = 0, q_elems = 0;
-    int zvariant = GNSS_ZVARIANT_AUTO;            // z kernel choice (gnss_set_option)
+    int zvariant = GNSS_VARIANT_AUTO;             // z kernel choice (gnss_set_option)
+    int pvariant = GNSS_VARIANT_AUTO;             // x / y pass kernel choice
     long long n_sphere = 0;                       // kept-box modes inside the dealiasing sphere
     int n_xin = 0;                                // x-inverse inputs (state fields; s twice with alpha)
     signed char xvar_in[6]{}, xvar_n[6]{}, xvar_mul[6][2]{}, xvar_out[6][2]{};
@@ -162,7 +168,23 @@ template <class K> static int blocks_per_sm(K kern, int threads, int smem) {
 
 template <typename T, int N> struct Launch {
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
-                            cudaStream_t s) {
+                            cudaStream_t s, int pvariant) {
+        if constexpr (N == 256 || N == 512) {
+            if (pvariant == GNSS_VARIANT_REGISTER) {   // register-resident column transforms (on request)
+                using C = PRCfg<T, N>;
+                auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;
+                cudaError_t e = prep_smem(kern, C::SMEM);
+                if (e != cudaSuccess) return e;
+                static int per_sm[2] = {0, 0};
+                int &ps = per_sm[sign < 0 ? 0 : 1];
+                if (ps == 0) ps = blocks_per_sm(kern, C::NT, C::SMEM);
+                const long long nitems = (long long)sp.nin * sp.outer.count() * sp.ncolblk;
+                long long grid = (long long)ps * nsm;
+                if (grid > nitems) grid = nitems;
+                kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(P, sp, reinterpret_cast<const V2<T> *>(tw));
+                return cudaGetLastError();
+            }
+        }
         using C = PassCfg<T, N>;
         auto kern = sign < 0 ? k_pass<T, N, -1> : k_pass<T, N, +1>;
         cudaError_t e = prep_smem(kern, C::SMEM);
@@ -249,7 +271,7 @@ template <typename T, int N> struct Launch {
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
                              unsigned *err, int nsm, cudaStream_t s, int zvariant) {
-        if (zvariant != GNSS_ZVARIANT_STAGED && zreg_fits(nph, nraw, ncp)) {
+        if (zvariant != GNSS_VARIANT_STAGED && zreg_fits(nph, nraw, ncp)) {
             if (nph == 9 && nraw == 10)
                 return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
             if (nph == 12 && nraw == 13)
@@ -288,8 +310,8 @@ template <typename T, int N> struct Launch {
 
 template <typename T>
 static cudaError_t launch_pass(int n, int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
-                               cudaStream_t s) {
-    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::pass(sign, P, sp, tw, nsm, s)));
+                               cudaStream_t s, int pvariant) {
+    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::pass(sign, P, sp, tw, nsm, s, pvariant)));
 }
 template <typename T>
 static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfields, long long nlines, int nz2, T scale,
@@ -473,10 +495,10 @@ template <typename T> static gnss_status forward_t(gnss_ctx *c, void *f, cudaStr
     PassPtrs<T> P{};
     P.in[0] = F.p[0];
     P.out[0] = X;
-    CK(c, launch_pass<T>(g.ny, -1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s));
+    CK(c, launch_pass<T>(g.ny, -1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s, c->pvariant));
     P.in[0] = X;
     P.out[0] = F.p[0];
-    CK(c, launch_pass<T>(g.nx, -1, P, pass_spec<T>(c, X_FWD, 1), c->tw[0], c->nsm, s));
+    CK(c, launch_pass<T>(g.nx, -1, P, pass_spec<T>(c, X_FWD, 1), c->tw[0], c->nsm, s, c->pvariant));
     return GNSS_OK;
 }
 
@@ -493,10 +515,10 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
     PassPtrs<T> P{};
     P.in[0] = F.p[0];
     P.out[0] = X;
-    CK(c, launch_pass<T>(g.nx, +1, P, pass_spec<T>(c, X_INV, 1), c->tw[0], c->nsm, s));
+    CK(c, launch_pass<T>(g.nx, +1, P, pass_spec<T>(c, X_INV, 1), c->tw[0], c->nsm, s, c->pvariant));
     P.in[0] = X;
     P.out[0] = F.p[0];
-    CK(c, launch_pass<T>(g.ny, +1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s));
+    CK(c, launch_pass<T>(g.ny, +1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s, c->pvariant));
     CK(c, launch_zpass<T>(g.nz, +1, F, 1, nlines, g.nz2, scale, c->tw[2], s));
     return GNSS_OK;
 }
@@ -545,7 +567,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             spx.nvar[i] = c->xvar_n[i];
             for (int v = 0; v < 2; ++v) { spx.vmul[i][v] = c->xvar_mul[i][v]; spx.vout[i][v] = c->xvar_out[i][v]; }
         }
-        CK(c, launch_pass<T>(g.nx, +1, P, spx, c->tw[0], c->nsm, s));
+        CK(c, launch_pass<T>(g.nx, +1, P, spx, c->tw[0], c->nsm, s, c->pvariant));
     }
     {
         StageTimer t(c, s, 1);
@@ -557,7 +579,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             spy.nvar[i] = c->yvar_n[i];
             for (int v = 0; v < 2; ++v) { spy.vmul[i][v] = c->yvar_mul[i][v]; spy.vout[i][v] = c->yvar_out[i][v]; }
         }
-        CK(c, launch_pass<T>(g.ny, +1, P, spy, c->tw[1], c->nsm, s));
+        CK(c, launch_pass<T>(g.ny, +1, P, spy, c->tw[1], c->nsm, s, c->pvariant));
     }
     {
         StageTimer t(c, s, 2);
@@ -568,13 +590,13 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
         StageTimer t(c, s, 3);
         PassPtrs<T> P{};
         for (int q = 0; q < nnl; ++q) { P.in[q] = Qf(q); P.out[q] = Pf(q); }
-        CK(c, launch_pass<T>(g.ny, -1, P, step_spec<T>(c, Y_FWD_STEP, nnl), c->tw[1], c->nsm, s));
+        CK(c, launch_pass<T>(g.ny, -1, P, step_spec<T>(c, Y_FWD_STEP, nnl), c->tw[1], c->nsm, s, c->pvariant));
     }
     {
         StageTimer t(c, s, 4);
         PassPtrs<T> P{};
         for (int q = 0; q < nnl; ++q) { P.in[q] = Pf(q); P.out[q] = R.p[q]; }
-        CK(c, launch_pass<T>(g.nx, -1, P, step_spec<T>(c, X_FWD_STEP, nnl), c->tw[0], c->nsm, s));
+        CK(c, launch_pass<T>(g.nx, -1, P, step_spec<T>(c, X_FWD_STEP, nnl), c->tw[0], c->nsm, s, c->pvariant));
     }
     {
         StageTimer t(c, s, 5);
@@ -662,8 +684,75 @@ template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields 
     return GNSS_OK;
 }
 
+// calcTurbStats_mgpu (statistics.cu:2039-2156): spectral sums, |omega| through
+// three inverse transforms of the vorticity (scratch fields 1..3; field 0 is
+// the transforms' own scratch), mean profiles from the kx = kz = 0 modes.
+template <typename T>
+static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *out, double *yprof, cudaStream_t s) {
+    const Geom &g = c->g;
+    const size_t nvals = TURB_SUMS + 1 + 5 * (size_t)g.ny;
+    if (!c->turb_part) {
+        if (cudaMalloc(&c->turb_part, sizeof(double) * STAT_BLOCKS * TURB_SUMS) != cudaSuccess ||
+            cudaMalloc(&c->turb_dev, sizeof(double) * nvals) != cudaSuccess ||
+            cudaMallocHost(&c->turb_host, sizeof(double) * nvals) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GNSS_ERR_NOMEM, "cannot allocate statistics buffers");
+        }
+        c->owned_bytes += sizeof(double) * (STAT_BLOCKS * TURB_SUMS + nvals);
+    }
+    gnss_status stt = ensure_scratch(c, 4);
+    if (stt) return stt;
+    FieldSet<T> F{};
+    void *sp[5] = {st->u, st->v, st->w, st->s, st->c};
+    for (int q = 0; q < 5; ++q) F.p[q] = reinterpret_cast<V2<T> *>(sp[q]);
+    c->launches += 2;
+    k_turb_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(F, st->s != nullptr, g, c->turb_part);
+    LAUNCH_CK(c);
+    k_sums_final<TURB_SUMS><<<1, TURB_SUMS * 32, 0, s>>>(c->turb_part, STAT_BLOCKS, TURB_SUMS, c->turb_dev);
+    LAUNCH_CK(c);
+    V2<T> *o[3];
+    for (int q = 0; q < 3; ++q) o[q] = fld<T>(c->scratch, c->nspec, 1 + q);
+    c->launches++;
+    k_vorticity<T><<<grid_for((long long)c->nspec, 256), 256, 0, s>>>(F.p[0], F.p[1], F.p[2], o[0], o[1], o[2], g);
+    LAUNCH_CK(c);
+    for (int q = 0; q < 3; ++q) {
+        gnss_status e = inverse_t<T>(c, o[q], s);
+        if (e) return e;
+    }
+    c->launches += 3;
+    k_absvort_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(reinterpret_cast<const T *>(o[0]),
+                                                               reinterpret_cast<const T *>(o[1]),
+                                                               reinterpret_cast<const T *>(o[2]), g, c->turb_part);
+    LAUNCH_CK(c);
+    k_sums_final<1><<<1, 32, 0, s>>>(c->turb_part, STAT_BLOCKS, TURB_SUMS, c->turb_dev + TURB_SUMS);
+    LAUNCH_CK(c);
+    k_yprof<T><<<5, 256, 0, s>>>(F, g, reinterpret_cast<const V2<T> *>(c->tw[1]), c->turb_dev + TURB_SUMS + 1);
+    LAUNCH_CK(c);
+    CK(c, cudaMemcpyAsync(c->turb_host, c->turb_dev, sizeof(double) * nvals, cudaMemcpyDeviceToHost, s));
+    CK(c, cudaStreamSynchronize(s));
+    gnss_status chk = gnss_check(c, s);
+    if (chk) return chk;
+    const gnss_config &k = c->cfg;
+    const double nn = (double)k.nx * k.ny * k.nz, n2 = nn * nn, nu = k.nu_stats;
+    const double *h = c->turb_host;
+    out->ke = (h[0] / n2) / 2.0;
+    out->vrms = std::sqrt((h[0] / n2) / 3.0);
+    out->epsilon = nu * (h[1] / n2);
+    out->eta = std::sqrt(std::sqrt(nu * nu * nu / out->epsilon));
+    out->l = 3 * M_PI / 4 * (h[2] / n2) / out->ke;
+    out->lambda = std::sqrt(15.0 * nu * out->vrms * out->vrms / out->epsilon);
+    out->chi = st->s ? 2.0 * (nu / k.sc) * (h[3] / n2) : 0.0;
+    out->omega_x = std::sqrt(h[4] / n2);
+    out->omega_y = std::sqrt(h[5] / n2);
+    out->omega_z = std::sqrt(h[6] / n2);
+    out->omega = h[TURB_SUMS] / nn;
+    if (yprof) std::memcpy(yprof, h + TURB_SUMS + 1, sizeof(double) * 5 * (size_t)g.ny);
+    return GNSS_OK;
+}
+
 // ============================================================== C ABI
 // (C linkage comes from the declarations in gnss_b200.h)
+
 
 const char *gnss_status_string(gnss_status st) {
     switch (st) {
@@ -716,22 +805,19 @@ gnss_status gnss_stage_bytes(const gnss_ctx *c, double *bytes) {
 
 gnss_status gnss_set_option(gnss_ctx *c, int key, int value) {
     if (!c) return GNSS_ERR_INVALID;
-    if (key == GNSS_OPT_ZVARIANT) {
-        if (value < GNSS_ZVARIANT_AUTO || value > GNSS_ZVARIANT_STAGED)
-            return fail(c, GNSS_ERR_INVALID, "bad z variant %d", value);
-        c->zvariant = value;
-        return GNSS_OK;
-    }
-    return fail(c, GNSS_ERR_INVALID, "unknown option %d", key);
+    if (key != GNSS_OPT_ZVARIANT && key != GNSS_OPT_PVARIANT) return fail(c, GNSS_ERR_INVALID, "unknown option %d", key);
+    if (value < GNSS_VARIANT_AUTO || value > GNSS_VARIANT_STAGED)
+        return fail(c, GNSS_ERR_INVALID, "bad variant %d for option %d", value, key);
+    (key == GNSS_OPT_ZVARIANT ? c->zvariant : c->pvariant) = value;
+    return GNSS_OK;
 }
 
 gnss_status gnss_get_option(const gnss_ctx *c, int key, int *value) {
     if (!c || !value) return GNSS_ERR_INVALID;
-    if (key == GNSS_OPT_ZVARIANT) {
-        *value = c->zvariant;
-        return GNSS_OK;
-    }
-    return GNSS_ERR_INVALID;
+    if (key == GNSS_OPT_ZVARIANT) *value = c->zvariant;
+    else if (key == GNSS_OPT_PVARIANT) *value = c->pvariant;
+    else return GNSS_ERR_INVALID;
+    return GNSS_OK;
 }
 
 gnss_status gnss_profile_enable(gnss_ctx *c, int on) {
@@ -987,6 +1073,9 @@ gnss_status gnss_destroy(gnss_ctx *c) {
     if (c->stat_part) cudaFree(c->stat_part);
     if (c->stat_dev) cudaFree(c->stat_dev);
     if (c->stat_host) cudaFreeHost(c->stat_host);
+    if (c->turb_part) cudaFree(c->turb_part);
+    if (c->turb_dev) cudaFree(c->turb_dev);
+    if (c->turb_host) cudaFreeHost(c->turb_host);
     if (c->d_err) cudaFree(c->d_err);
     if (c->res) cudaFree(c->res);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -995,6 +1084,14 @@ gnss_status gnss_destroy(gnss_ctx *c) {
 }
 
 #define PREC_CALL(c, fn, ...) ((c)->cfg.precision == GNSS_FP64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+gnss_status gnss_turb_stats(gnss_ctx *c, const gnss_fields *state, gnss_turb *out, double *yprof, void *stream) {
+    if (!c || !state || !out || !state->u || !state->v || !state->w)
+        return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!al_fields(c, state)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
+    CK(c, cudaSetDevice(c->cfg.device));
+    return PREC_CALL(c, turb_stats_t, c, state, out, yprof, S(stream));
+}
 
 gnss_status gnss_forward(gnss_ctx *c, void *f, void *stream) {
     if (!c || !f) return fail(c, GNSS_ERR_INVALID, "null argument");

@@ -1,0 +1,156 @@
+// passreg.cuh -- strided x / y passes with register-resident column
+// transforms (N = 256, 512).
+//
+// Same contract as k_pass (PassSpec / PassPtrs: tiles of NB columns x N rows,
+// kept / compact rows and outer indices, up to two outputs per tile, each the
+// transform of the tile times a spectral multiplier, optional dealias mask),
+// with a different schedule: warp w owns column w of the tile and transforms
+// it in registers with zr_fft (one transpose through its own scratch), so a
+// column crosses shared memory three times (load, transpose, store) and the
+// block synchronises per tile and per output instead of per radix stage.
+//   tile rows are padded to NB + 1 elements: a warp reading one column and a
+//   half-warp pair writing one row are both free of bank conflicts;
+//   the next tile is copied with cp.async (rows the spec does not keep are
+//   neither copied nor read) while the current one is transformed;
+//   the dealias mask keeps rows whose |index| is at most a bound computed
+//   once per tile and column (k^2 grows with |k_row|), with the reference's
+//   test k^2 > kmax^2 (solver.cu:36) evaluated in the reference's order;
+//   results go through the consumed input buffer to coalesced row stores.
+#pragma once
+#include "zreg.cuh"
+
+namespace gnss {
+
+template <typename T, int N> struct PRCfg {
+    using Z = ZRCfg<T, N>;
+    static constexpr int NB = PassCfg<T, N>::NB;          // columns per tile (as k_pass) = warps per block
+    static constexpr int NT = NB * 32;
+    static constexpr int LD = NB + 1;                     // padded row
+    static constexpr int TILE = N * LD;
+    static constexpr int SMEM = (2 * TILE + NB * Z::SCR + Z::LOGE * 32) * (int)sizeof(V2<T>);
+};
+
+// |row index| of a transform row (the Nyquist row counts as N/2)
+template <int N> __device__ __forceinline__ int row_dist(int r) { return r <= N / 2 ? r : N - r; }
+
+template <typename T, int N, int SIGN>
+__global__ void __launch_bounds__(PRCfg<T, N>::NT, 1)
+k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec sp, const V2<T> *__restrict__ tw) {
+    using V = V2<T>;
+    using C = PRCfg<T, N>;
+    using Z = ZRCfg<T, N>;
+    constexpr int NB = C::NB, NT = C::NT, LD = C::LD, TILE = C::TILE, E = Z::E;
+    constexpr int RSTEP = NT / NB;   // rows per copy sweep (32)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tiles = reinterpret_cast<V *>(smem_raw);
+    V *scr_all = tiles + 2 * TILE;
+    V *tws = scr_all + NB * Z::SCR;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = sp.outer.count() * sp.ncolblk;
+    const long long nitems = (long long)sp.nin * ntiles;
+    long long item = blockIdx.x;
+    if (item >= nitems) return;
+    for (int i = tid; i < Z::LOGE * 32; i += NT) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
+        fi = (int)(it / ntiles);
+        const int t = (int)(it % ntiles);
+        oc = t / sp.ncolblk;
+        o = sp.outer.expand(oc);
+        c0 = (t % sp.ncolblk) * NB;
+    };
+    // copy of one tile: thread -> column tid % NB, rows tid / NB + 32 k (kept rows only)
+    auto prefetch = [&](long long it, V *dst) {
+        int fi, oc, o, c0;
+        decode(it, fi, oc, o, c0);
+        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        const int b = tid % NB;
+        if (c0 + b >= sp.ncols) return;
+#pragma unroll 4
+        for (int row = tid / NB; row < N; row += RSTEP) {
+            if (!sp.row_in.kept(row)) continue;
+            const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
+            const V *p = src + (long long)r * sp.s_row + b;
+            if constexpr (sizeof(T) == 8) cp_async16(dst + row * LD + b, p, 16);
+            else cp_async8(dst + row * LD + b, p, 8);
+        }
+    };
+    prefetch(item, tiles);
+    cp_async_commit();
+    V *scr = scr_all + warp * Z::SCR;
+    int buf = 0;
+    for (; item < nitems; item += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();   // current tile landed; the other buffer's last readers are done
+        const long long next = item + gridDim.x;
+        if (next < nitems) prefetch(next, tiles + (buf ^ 1) * TILE);
+        cp_async_commit();
+        int fi, oc, o, c0;
+        decode(item, fi, oc, o, c0);
+        V *cur = tiles + buf * TILE;
+        const int b = warp;                       // this warp's column
+        const bool col_ok = c0 + b < sp.ncols;
+        const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
+        const double kc = wavenum(c0 + b, sp.n_col, sp.dk_col);
+        // rows kept by the dealias mask: |row index| <= dmax (prefix by monotonicity of k^2)
+        int dmax = N;
+        if (sp.mask) {
+            int cnt = 0;
+            for (int d0 = 0; d0 <= N / 2; d0 += 32) {
+                const int d = d0 + lane;
+                const bool ok = d <= N / 2 && !(ksq3(sp.dk_row * (double)d, k_out, kc) > sp.kmax2);
+                cnt += __popc(__ballot_sync(0xffffffffu, ok));
+            }
+            dmax = cnt - 1;
+        }
+        V a[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int row = lane + 32 * m;
+            const bool ok = col_ok && sp.row_in.kept(row) && row_dist<N>(row) <= dmax;
+            a[m] = ok ? cur[row * LD + b] : V{T(0), T(0)};
+        }
+        __syncthreads();   // tile consumed: `cur` becomes the output tile
+        const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const int out_cols = sp.out_ncols - c0;
+        const int nv = sp.nvar[fi];
+        for (int v = 0; v < nv; ++v) {
+            const int mul = sp.vmul[fi][v];
+            V x[E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const V q = a[m];
+                if (mul == V_ONE) {
+                    x[m] = q;
+                } else {
+                    const double kr = wavenum(lane + 32 * m, sp.n_row, sp.dk_row);
+                    if (mul == V_IK_ROW) x[m] = V{(T)(-kr) * q.y, (T)kr * q.x};
+                    else if (mul == V_IK_OUT) x[m] = V{(T)(-k_out) * q.y, (T)k_out * q.x};
+                    else if (mul == V_IK_COL) x[m] = V{(T)(-kc) * q.y, (T)kc * q.x};
+                    else {   // V_LAP
+                        const T k2 = (T)ksq3(kr, k_out, kc);
+                        x[m] = V{-k2 * q.x, -k2 * q.y};
+                    }
+                }
+            }
+            zr_fft<T, N, SIGN>(lane, x, scr, tws);
+#pragma unroll
+            for (int q = 0; q < E; ++q) cur[zr_out_index<T, N>(lane, q) * LD + b] = x[q];
+            __syncthreads();   // output tile complete
+            V *dst = P.out[sp.vout[fi][v]] + dbase;
+            const int bb = tid % NB;
+            if (bb < out_cols) {
+                const int nrow = sp.row_out.count();
+                for (int rc = tid / NB; rc < nrow; rc += RSTEP) {
+                    const int row = sp.row_out.expand(rc);
+                    const int r = sp.row_out_compact ? rc : row;
+                    dst[(long long)r * sp.d_row + bb] = cur[row * LD + bb];
+                }
+            }
+            if (v + 1 < nv) __syncthreads();   // output tile free for the next output
+        }
+        buf ^= 1;
+    }
+    cp_async_wait<0>();
+}
+
+}  // namespace gnss

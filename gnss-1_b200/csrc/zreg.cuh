@@ -138,23 +138,34 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
     constexpr int E = Z::E, G = Z::G, S = Z::S;
     Dft<E, SIGN, V>::run(x);
     {
-        V w[E];
-#pragma unroll
-        for (int b = 0; b < Z::LOGE; ++b) {
+        // W^k1 for k1 = 1, 2, 4 (, 8) from the table, the others as products
+        // (w3 = w1 w2, w5 = w1 w4, w6 = w2 w4, w7 = w3 w4, w(8+i) = w(i) w8),
+        // each applied as soon as it is formed
+        auto tw_at = [&](int b) {
             V t = tws[32 * b + lane];
             if (SIGN > 0) t.y = -t.y;
-            w[1 << b] = t;
-        }
-        w[3] = cmul(w[1], w[2]);
-        w[5] = cmul(w[1], w[4]);
-        w[6] = cmul(w[2], w[4]);
-        w[7] = cmul(w[3], w[4]);
+            return t;
+        };
+        const V w1 = tw_at(0), w2 = tw_at(1), w4 = tw_at(2);
+        const V w3 = cmul(w1, w2);
         if constexpr (E == 16) {
-#pragma unroll
-            for (int i = 1; i < 8; ++i) w[8 + i] = cmul(w[i], w[8]);
+            const V w8 = tw_at(3);
+            x[8] = cmul(x[8], w8);
+            x[9] = cmul(x[9], cmul(w1, w8));
+            x[10] = cmul(x[10], cmul(w2, w8));
+            x[11] = cmul(x[11], cmul(w3, w8));
+            x[12] = cmul(x[12], cmul(w4, w8));
+            x[13] = cmul(x[13], cmul(cmul(w1, w4), w8));
+            x[14] = cmul(x[14], cmul(cmul(w2, w4), w8));
+            x[15] = cmul(x[15], cmul(cmul(w3, w4), w8));
         }
-#pragma unroll
-        for (int k1 = 1; k1 < E; ++k1) x[k1] = cmul(x[k1], w[k1]);
+        x[1] = cmul(x[1], w1);
+        x[2] = cmul(x[2], w2);
+        x[3] = cmul(x[3], w3);
+        x[4] = cmul(x[4], w4);
+        x[5] = cmul(x[5], cmul(w1, w4));
+        x[6] = cmul(x[6], cmul(w2, w4));
+        x[7] = cmul(x[7], cmul(w3, w4));
     }
 #pragma unroll
     for (int k1 = 0; k1 < E; ++k1) scr[k1 * S + lane] = x[k1];

@@ -33,9 +33,10 @@ GNSS_FP64 = 0
 GNSS_FP32 = 1
 GNSS_NSTATS = 7
 GNSS_OPT_ZVARIANT = 0
-GNSS_ZVARIANT_AUTO = 0
-GNSS_ZVARIANT_REGISTER = 1
-GNSS_ZVARIANT_STAGED = 2
+GNSS_OPT_PVARIANT = 1
+GNSS_VARIANT_AUTO = GNSS_ZVARIANT_AUTO = 0
+GNSS_VARIANT_REGISTER = GNSS_ZVARIANT_REGISTER = 1
+GNSS_VARIANT_STAGED = GNSS_ZVARIANT_STAGED = 2
 STAT_NAMES = ("ke", "vrms2", "eps", "chi_s", "chi_c", "var_s", "var_c")
 SUPPORTED_SIZES = (8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512)
 
@@ -56,6 +57,11 @@ class GnssConfig(ctypes.Structure):
         ("n_scalars", ctypes.c_int), ("scheme", ctypes.c_int), ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
     ]
+
+
+class GnssTurb(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("vrms", "ke", "epsilon", "eta", "l", "lambda_", "chi", "omega",
+                                               "omega_x", "omega_y", "omega_z")]
 
 
 class GnssFields(ctypes.Structure):
@@ -97,6 +103,7 @@ _SIGS = {
     "gnss_get_option": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
     "gnss_scratch_bytes": [_VP],
+    "gnss_turb_stats": [_VP, ctypes.POINTER(GnssFields), _VP, ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_attach_scratch": [_VP, _VP, ctypes.c_size_t],
     "gnss_ensemble_create": [ctypes.POINTER(GnssConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
     "gnss_ensemble_destroy": [_VP],
@@ -360,6 +367,18 @@ class Context:
     # -- instrumentation ------------------------------------------------------
     def launch_count(self) -> int:
         return int(self.lib.gnss_launch_count(self._h))
+
+    def turb_stats(self, state: Sequence, profiles: bool = True, stream=None):
+        """calcTurbStats_mgpu (statistics.cu:2039-2156): (dict, mean y-profiles [5, ny] of u, v, w, s, c)."""
+        t = GnssTurb()
+        prof = np.zeros((5, self.cfg.ny)) if profiles else None
+        pp = prof.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if prof is not None else None
+        f = _fields(state)
+        self._ck(self.lib.gnss_turb_stats(self._h, ctypes.byref(f), ctypes.byref(t), pp, _stream(stream)),
+                 "gnss_turb_stats")
+        d = {k: getattr(t, k) for k, _ in GnssTurb._fields_}
+        d["lambda"] = d.pop("lambda_")
+        return d, prof
 
     def set_option(self, key: int, value: int) -> None:
         self._ck(self.lib.gnss_set_option(self._h, key, value), "gnss_set_option")

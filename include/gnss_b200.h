@@ -154,6 +154,26 @@ gnss_status gnss_step(gnss_ctx *ctx, const gnss_fields *state, const gnss_fields
  * calcScalarDissipationRate: statistics.cu:1494-1845). */
 gnss_status gnss_stats(gnss_ctx *ctx, const gnss_fields *state, double *out, void *stream);
 
+/* Turbulence statistics of a state (calcTurbStats_mgpu, statistics.cu:2039-2156),
+ * with the reference's definitions (nu = cfg.nu_stats):
+ *   vrms     sqrt(sum |u_hat|^2 / (3 NN^2))                     (calcVrms, :1551, 1582)
+ *   ke       1/2 sum |u_hat|^2 / NN^2                           (:1549)
+ *   epsilon  nu sum k^2 |u_hat|^2 / NN^2                        (calcEpsilonKernel_mgpu)
+ *   eta      (nu^3 / epsilon)^(1/4)                             (:2149)
+ *   l        3 pi/4 sum_{k != 0} |u_hat|^2/(2 |k| NN^2) / ke    (calcIntegralLength, :2150)
+ *   lambda   sqrt(15 nu vrms^2 / epsilon)                       (:2148)
+ *   chi      2 nu/sc sum k^2 |s_hat|^2 / NN^2                    (calcScalarDissipationRate)
+ *   omega    volume average of |curl u|                         (:2097-2106)
+ *   omega_x, omega_y, omega_z  rms of each vorticity component (:2103-2105)
+ * Sums run over the full spectrum (kz mirror) in a fixed order.  yprof (may
+ * be NULL) receives 5 x ny doubles: the mean profiles along y (averages over
+ * x and z) of u, v, w, s, c (zeros for a missing c) (calcYprof, :1943-2003).
+ * Uses four scratch fields of the context; synchronises the stream. */
+typedef struct gnss_turb {
+    double vrms, ke, epsilon, eta, l, lambda, chi, omega, omega_x, omega_y, omega_z;
+} gnss_turb;
+gnss_status gnss_turb_stats(gnss_ctx *ctx, const gnss_fields *state, gnss_turb *out, double *yprof, void *stream);
+
 /* End-to-end call with host buffers: copies the packed host state
  * (3 + n_scalars spectral fields back to back) to context-owned device
  * buffers, dealiases it (main.cu:156), runs n_steps steps (the first one
@@ -191,16 +211,24 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 
 /* Kernel variant options of a context (the knobs the autotuner sets; no
  * counterpart in the reference, which has one cuFFT plan per size).
- * GNSS_OPT_ZVARIANT picks the kernel of the fused z stage:
- *   GNSS_ZVARIANT_AUTO      register-resident line transforms where they
- *                           exist (N = 256, 512) and fit, else staged;
- *   GNSS_ZVARIANT_REGISTER  the same as AUTO (a request, not a guarantee);
- *   GNSS_ZVARIANT_STAGED    per-stage line transforms through shared memory.
+ * GNSS_OPT_ZVARIANT picks the kernel of the fused z stage, GNSS_OPT_PVARIANT
+ * the kernel of the strided x and y passes (of the step and of the 3D
+ * transforms):
+ *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
+ *                          resident line transforms for the z stage where
+ *                          they exist (N = 256, 512) and fit, staged passes;
+ *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
+ *                          (N = 256, 512) and fit (a request, not a guarantee);
+ *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory.
  * Every variant computes the same step to round-off. */
 #define GNSS_OPT_ZVARIANT 0
-#define GNSS_ZVARIANT_AUTO 0
-#define GNSS_ZVARIANT_REGISTER 1
-#define GNSS_ZVARIANT_STAGED 2
+#define GNSS_OPT_PVARIANT 1
+#define GNSS_VARIANT_AUTO 0
+#define GNSS_VARIANT_REGISTER 1
+#define GNSS_VARIANT_STAGED 2
+#define GNSS_ZVARIANT_AUTO GNSS_VARIANT_AUTO
+#define GNSS_ZVARIANT_REGISTER GNSS_VARIANT_REGISTER
+#define GNSS_ZVARIANT_STAGED GNSS_VARIANT_STAGED
 gnss_status gnss_set_option(gnss_ctx *ctx, int key, int value);
 gnss_status gnss_get_option(const gnss_ctx *ctx, int key, int *value);
 

@@ -649,4 +649,85 @@ int orc_stats(const orc_cfg *c, double **fields, double *out) {
     return 0;
 }
 
+/* calcTurbStats_mgpu (statistics.cu:2039-2156), in the reference's own
+ * form: spectral sums for Vrms, KE, epsilon, the integral length and chi
+ * (calcVrms, calcDissipationRate, calcIntegralLength,
+ * calcScalarDissipationRate); vorticity transformed to physical space for
+ * the rms of its components and the volume average of its magnitude
+ * (statistics.cu:2083-2106); the fields transformed to physical space and
+ * averaged over x and z for the mean profiles (calcYprof, :1943-2003);
+ * lambda, eta and l from the derived formulas (:2147-2150). */
+int orc_turb_stats(const orc_cfg *c, double **fields, double *out, double *yprof) {
+    if (!valid(c)) return 1;
+    Grid g(c);
+    const double NN = (double)g.nx * g.ny * g.nz;
+    const size_t nspec = (size_t)g.nx * g.ny * g.nz2;
+    double st[7];
+    orc_stats(c, fields, st);
+    const double ke = st[0];
+    const double vrms = std::sqrt(st[1]);                       /* statistics.cu:1582 */
+    const double eps = st[2];
+    const double chi = st[3];
+    long double sl = 0;                                          /* calcIntegralLengthKernel_mgpu */
+    const cpx *U = (const cpx *)fields[0], *V = (const cpx *)fields[1], *W = (const cpx *)fields[2];
+#pragma omp parallel for num_threads(nthreads_of(c)) reduction(+ : sl) schedule(static)
+    for (int j = 0; j < g.ny; ++j)
+        for (int i = 0; i < g.nx; ++i)
+            for (int k = 0; k < g.nz2; ++k) {
+                const size_t id = k + (size_t)g.nz2 * (i + (size_t)g.nx * j);
+                const double wgt = (k == 0 || 2 * k == g.nz) ? 1.0 : 2.0;
+                const double ksq = g.kx[i] * g.kx[i] + g.ky[j] * g.ky[j] + g.kz[k] * g.kz[k];
+                if (ksq > 0) {
+                    const double e = (U[id].re * U[id].re + U[id].im * U[id].im) / (NN * NN) +
+                                     (V[id].re * V[id].re + V[id].im * V[id].im) / (NN * NN) +
+                                     (W[id].re * W[id].re + W[id].im * W[id].im) / (NN * NN);
+                    sl += wgt * e / (2.0 * std::sqrt(ksq));
+                }
+            }
+    /* vorticity in physical space (vorticity + inverseTransform, :2079-2092) */
+    std::vector<double> om[3];
+    for (auto &o : om) o.assign(2 * nspec, 0.0);
+    orc_vorticity(c, fields[0], fields[1], fields[2], om[0].data(), om[1].data(), om[2].data());
+    for (auto &o : om) orc_inverse(c, o.data());
+    long double s2[3] = {0, 0, 0}, smag = 0;
+    for (int i = 0; i < g.nx; ++i)
+        for (int j = 0; j < g.ny; ++j)
+            for (int k = 0; k < g.nz; ++k) {
+                const size_t id = k + 2 * (size_t)g.nz2 * (j + (size_t)g.ny * i);
+                const double a = om[0][id], b = om[1][id], d = om[2][id];
+                s2[0] += a * a / NN;                            /* volumeAverage_kernel type 1 */
+                s2[1] += b * b / NN;
+                s2[2] += d * d / NN;
+                smag += std::sqrt(a * a + b * b + d * d) / NN;   /* VectorMagnitude + type 0 */
+            }
+    out[0] = vrms;
+    out[1] = ke;
+    out[2] = eps;
+    out[3] = std::sqrt(std::sqrt(c->nu_stats * c->nu_stats * c->nu_stats / eps));   /* eta, :2149 */
+    out[4] = 3 * M_PI / 4 * (double)sl / ke;                                        /* l, :2150 */
+    out[5] = std::sqrt(15.0 * c->nu_stats * vrms * vrms / eps);                     /* lambda, :2148 */
+    out[6] = chi;
+    out[7] = (double)smag;
+    out[8] = std::sqrt((double)s2[0]);
+    out[9] = std::sqrt((double)s2[1]);
+    out[10] = std::sqrt((double)s2[2]);
+    if (yprof) {   /* calcYprof: sum over x and z of the physical field / (NX NZ) */
+        std::vector<double> f(2 * nspec);
+        for (int q = 0; q < 5; ++q) {
+            double *pr = yprof + (size_t)q * g.ny;
+            for (int j = 0; j < g.ny; ++j) pr[j] = 0.0;
+            if (!fields[q]) continue;
+            std::copy(fields[q], fields[q] + 2 * nspec, f.begin());
+            orc_inverse(c, f.data());
+            for (int j = 0; j < g.ny; ++j) {
+                long double acc = 0;
+                for (int i = 0; i < g.nx; ++i)
+                    for (int k = 0; k < g.nz; ++k) acc += f[k + 2 * (size_t)g.nz2 * (j + (size_t)g.ny * i)];
+                pr[j] = (double)(acc / ((double)g.nx * g.nz));
+            }
+        }
+    }
+    return 0;
+}
+
 } /* extern "C" */

@@ -61,6 +61,13 @@ int orc_step_rk3if(const orc_cfg *c, double **fields, double **hist, int n_scala
  * out[2]=epsilon, out[3]=chi_s, out[4]=chi_c, out[5]=var_s, out[6]=var_c. */
 int orc_stats(const orc_cfg *c, double **fields, double *out);
 
+/* Turbulence statistics of calcTurbStats_mgpu (statistics.cu:2039-2156):
+ * out[0]=Vrms, [1]=KE, [2]=epsilon, [3]=eta, [4]=l, [5]=lambda, [6]=chi,
+ * [7]=omega (mean |vorticity|), [8..10]=rms of the vorticity components;
+ * yprof (may be NULL): 5 x ny mean profiles along y of fields[0..4]
+ * (zero for a NULL field). */
+int orc_turb_stats(const orc_cfg *c, double **fields, double *out, double *yprof);
+
 /* plain batched complex FFT for unit tests: data [n][batch] interleaved complex */
 int orc_fft_c2c(int n, int batch, double *data, int sign);
 

@@ -58,6 +58,7 @@ def lib():
             ("orc_step_cnab2", [C, PP, PP, ctypes.c_int]),
             ("orc_step_rk3if", [C, PP, PP, ctypes.c_int]),
             ("orc_stats", [C, PP, P]),
+            ("orc_turb_stats", [C, PP, P, P]),
             ("orc_fft_c2c", [ctypes.c_int, ctypes.c_int, P, ctypes.c_int]),
         ]:
             f = getattr(L, name)
@@ -159,3 +160,16 @@ def fft_c2c(x: np.ndarray, sign: int) -> np.ndarray:
 
 def nthreads_default() -> int:
     return os.cpu_count() or 1
+
+
+TURB_NAMES = ("vrms", "ke", "epsilon", "eta", "l", "lambda", "chi", "omega", "omega_x", "omega_y", "omega_z")
+
+
+def turb_stats(c: OrcCfg, fields, with_profiles: bool = True):
+    """calcTurbStats_mgpu restated: (dict of TURB_NAMES, profiles [5][ny] or None)."""
+    arr = _pp(list(fields) + [None] * (5 - len(fields)))
+    out = (ctypes.c_double * 11)()
+    prof = np.zeros((5, c.ny)) if with_profiles else None
+    pp = prof.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if prof is not None else None
+    _check(lib().orc_turb_stats(ctypes.byref(c), arr, out, pp), "turb_stats")
+    return {k: float(out[i]) for i, k in enumerate(TURB_NAMES)}, prof

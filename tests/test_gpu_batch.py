@@ -26,11 +26,12 @@ def _init(G, cfg, seed):
     return G.pack_state(f)
 
 
-def _alone(G, cfg, packed, steps, zvariant=None):
+def _alone(G, cfg, packed, steps, choice=None):
     kw = {k: getattr(cfg, k) for k, _ in G.GnssConfig._fields_ if k not in ("nx", "ny", "nz")}
     with G.Context(nx=cfg.nx, ny=cfg.ny, nz=cfg.nz, **kw) as ctx:
-        if zvariant is not None:
-            ctx.set_option(G.GNSS_OPT_ZVARIANT, zvariant)
+        if choice is not None:   # autotuner choice: z variant + 4 * pass variant
+            ctx.set_option(G.GNSS_OPT_ZVARIANT, choice & 3)
+            ctx.set_option(G.GNSS_OPT_PVARIANT, choice >> 2)
         out = np.empty_like(packed)
         stats = np.zeros((steps, G.GNSS_NSTATS))
         ctx.run_host(packed, out, steps, True, stats)
@@ -68,7 +69,8 @@ def test_ensemble_autotune_keeps_results(torch_cuda):
     init = [_init(G, c, seed=3 + i) for i, c in enumerate(cfgs)]
     with G.Ensemble(cfgs, n_branches=2) as ens:
         choices = ens.autotune(2)
-        assert all(ch in (G.GNSS_ZVARIANT_AUTO, G.GNSS_ZVARIANT_STAGED) for ch in choices)
+        allowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED)
+        assert all(ch & 3 in allowed and ch >> 2 in allowed for ch in choices)
         for i, a in enumerate(init):
             ens.upload(i, a)
         ens.step(4)
@@ -78,7 +80,7 @@ def test_ensemble_autotune_keeps_results(torch_cuda):
             ens.download(i, out)
             outs.append(out)
     for i, (c, a) in enumerate(zip(cfgs, init)):
-        ref, _ = _alone(G, c, a, 4, zvariant=choices[i])
+        ref, _ = _alone(G, c, a, 4, choice=choices[i])
         assert np.array_equal(outs[i], ref), f"member {i}"
 
 

@@ -1,12 +1,14 @@
-"""The two kernels of the fused z stage give the same step.
+"""The kernel variants of the step give the same step.
 
 At N = 256 and 512 the z stage runs register-resident line transforms
-(k_zreg); the staged kernel (k_zphys, per-stage transforms through shared
-memory) serves every size.  Both evaluate the nonlinear term of solver_ps
-(solver.cu:700-765); here one context steps the same dealiased state with
-each variant (gnss_set_option) and the fields must agree to round-off:
-relative L2 <= 1e-13 in FP64 and <= 2e-6 in FP32 after two steps.  The FP64
-register path is also held to the oracle at 256^3 (1e-12 after one step).
+(k_zreg) and the strided x / y passes register-resident column transforms
+(k_passr); the staged kernels (k_zphys, k_pass: per-radix-stage transforms
+through shared memory) serve every size.  All evaluate the nonlinear term of
+solver_ps (solver.cu:700-765); here one context steps the same dealiased
+state with every combination of the two options (gnss_set_option) and the
+fields must agree to round-off: relative L2 <= 1e-13 in FP64 and <= 2e-6 in
+FP32 after two steps.  The FP64 register path is also held to the oracle at
+256^3 (1e-12 after one step).
 """
 import numpy as np
 import pytest
@@ -23,8 +25,9 @@ CASES = [
 ]
 
 
-def _run(G, torch, ctx, init, steps, variant):
+def _run(G, torch, ctx, init, steps, variant, pvariant=0):
     ctx.set_option(G.GNSS_OPT_ZVARIANT, variant)
+    ctx.set_option(G.GNSS_OPT_PVARIANT, pvariant)
     st = [to_dev(torch, a) for a in init]
     hi = [torch.zeros_like(st[0]) for _ in st]
     ctx.de_alias(st)
@@ -45,12 +48,14 @@ def test_register_and_staged_z_agree(torch_cuda, n, precision, ns, alpha):
     cdt = np.complex128 if precision == 0 else np.complex64
     init = G.jet_initial_state(n, n_scalars=ns, seed=5, noise_kmax=8.0, amp=0.05, dtype=cdt)
     tol = 1e-13 if precision == 0 else 2e-6
+    A, S = G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED
     with G.Context(n, re=3000.0, sc=0.7, sc_c=1.0, alpha=alpha, dt=5e-4, n_scalars=ns, precision=precision) as ctx:
-        a = _run(G, torch, ctx, init, 2, G.GNSS_ZVARIANT_AUTO)
-        b = _run(G, torch, ctx, init, 2, G.GNSS_ZVARIANT_STAGED)
-    for q in range(3 + ns):
-        err = rel_l2(a[q], b[q])
-        assert err < tol, f"field {q}: register vs staged rel L2 {err:.3e}"
+        a = _run(G, torch, ctx, init, 2, A, A)
+        for zv, pv in ((S, A), (A, S), (S, S)):
+            b = _run(G, torch, ctx, init, 2, zv, pv)
+            for q in range(3 + ns):
+                err = rel_l2(a[q], b[q])
+                assert err < tol, f"z {zv} pass {pv} field {q}: rel L2 {err:.3e} against the register kernels"
 
 
 @pytest.mark.gpu
@@ -71,3 +76,27 @@ def test_register_z_matches_oracle_256(torch_cuda, oracle):
     for q in range(3 + ns):
         err = rel_l2(got[q], f[q])
         assert err < 1e-12, f"field {q}: rel L2 {err:.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(256, 256, 32), (512, 8, 16), (16, 512, 8)])
+def test_register_passes_in_the_3d_transforms(torch_cuda, oracle, shape):
+    """gnss_forward / gnss_inverse (fftfuncs.cu:288-359) with the register pass kernel, against the oracle."""
+    import gnss_b200 as G
+    from _util import buffer_to_phys, phys_to_buffer, rel_max
+    torch = torch_cuda
+    nx, ny, nz = shape
+    u = np.random.default_rng(17).standard_normal(shape)
+    buf = phys_to_buffer(u)
+    ref = buf.copy()
+    oc = oracle.cfg(nx=nx, ny=ny, nz=nz)
+    oracle.forward(oc, ref)
+    with G.Context(nx=nx, ny=ny, nz=nz) as ctx:
+        ctx.set_option(G.GNSS_OPT_PVARIANT, G.GNSS_VARIANT_REGISTER)
+        t = to_dev(torch, buf)
+        ctx.forward_transform(t)
+        torch.cuda.synchronize()
+        assert rel_max(to_host(t), ref) < 1e-13
+        ctx.inverse_transform(t)
+        torch.cuda.synchronize()
+        assert rel_max(buffer_to_phys(to_host(t), shape), u) < 1e-13
