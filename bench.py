@@ -130,13 +130,19 @@ def measured_peaks() -> dict:
 
 
 # ------------------------------------------------------------------ our arm
-def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None):
+VARIANTS = {"auto": 0, "register": 1, "staged": 2}
+
+
+def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None, variants=None):
     """Time `steps` steps of one jet resident on `dev`; returns a dict."""
     cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
     nx, ny, nz = (n, n, n) if isinstance(n, int) else n
     init = G.jet_initial_state(nx, ny, nz, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
     ctx = G.Context(nx=nx, ny=ny, nz=nz, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme,
                     device=dev)
+    if variants:
+        ctx.set_option(G.GNSS_OPT_ZVARIANT, VARIANTS[variants[0]])
+        ctx.set_option(G.GNSS_OPT_PVARIANT, VARIANTS[variants[1]])
     st = [torch.from_numpy(a.astype(cdt)).to(f"cuda:{dev}") for a in init]
     del init
     hi = [torch.zeros_like(st[0]) for _ in st] if scheme == G.GNSS_SCHEME_CNAB2 else None
@@ -367,13 +373,15 @@ def ours(args):
     scheme = G.GNSS_SCHEME_CNAB2 if args.scheme == "cnab2" else G.GNSS_SCHEME_RK3IF
     n = args.n
     shape = tuple(int(v) for v in args.grid.split("x")) if args.grid else (n, n, n)
-    leg = run_leg(G, torch, shape, prec, scheme, args.steps, args.warmup, dev, barrier=barrier)
+    var = (args.z_variant, args.pass_variant)
+    leg = run_leg(G, torch, shape, prec, scheme, args.steps, args.warmup, dev, barrier=barrier, variants=var)
     ms = leg["ms"] if red is None else red(leg["ms"])
     pts = float(shape[0] * shape[1] * shape[2])
     value = replica_value(pts, ms, ws)
     fp64 = None
     if prec == G.GNSS_FP32 and not args.no_fp64_leg:
-        l64 = run_leg(G, torch, shape, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier)
+        l64 = run_leg(G, torch, shape, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier,
+                      variants=var)
         ms64 = l64["ms"] if red is None else red(l64["ms"])
         fp64 = {"value": round(replica_value(pts, ms64, ws), 3), "ms_per_step": round(ms64, 4),
                 "mixed_over_fp64": round(ms64 / ms, 3),
@@ -437,6 +445,7 @@ def ours(args):
                                f"1 scalar, Re {RE:g}, Sc {SC}, dt {DT:g}, "
                                f"noise |k|<={NOISE_K:g} rms {AMP}, 2/3 dealias, {args.scheme}",
                    "grid": n, "precision": args.precision, "scheme": args.scheme,
+                   "kernels": {"z": args.z_variant, "pass": args.pass_variant},
                    "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (>= 0.5 GB per field); no flush"},
         "gpu_launches": leg["launches"], "clocks": leg["clocks"], "e2e": e2e, "roofline": roofline,
@@ -496,6 +505,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-leg", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--z-variant", choices=tuple(VARIANTS), default="auto")
+    ap.add_argument("--pass-variant", choices=tuple(VARIANTS), default="auto")
     ap.add_argument("--no-error-check", action="store_true")
     ap.add_argument("--error-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")

@@ -1,15 +1,16 @@
 // diag.cuh -- turbulence diagnostics of a spectral state (calcTurbStats_mgpu,
 // statistics.cu:2039-2156): the spectral sums behind Vrms, KE, epsilon, the
-// integral length and chi, the rms of each vorticity component, the volume
-// average of |omega| and the mean profiles along y.
+// integral length and chi, the rms of each vorticity component and the volume
+// average of |omega| over the grid, and the mean profiles along y.
 //
 // Spectral sums run over the full spectrum through the kz mirror (weight 1 on
 // kz = 0 and kz = nz/2, 2 elsewhere, as calcVrmsKernel_mgpu's kp = NZ - k
 // branch, statistics.cu:1505-1532), Kahan-compensated per thread and reduced
-// in a fixed order.  The rms of a vorticity component is the spectral sum of
-// |i k x u|^2 (Parseval; the reference averages the squares of the physical
-// field, statistics.cu:2103-2105).  |omega| itself has no spectral shortcut:
-// it is averaged over the physical vorticity (statistics.cu:2097-2106).  The
+// in a fixed order.  The vorticity statistics are taken, as in the
+// reference, over the physical vorticity (statistics.cu:2097-2106): a
+// spectral (Parseval) sum would differ from the grid average whenever
+// Nyquist modes survive the dealiasing (grids thinner than nx along y or z),
+// because the inverse transform drops their imaginary parts.  The
 // mean profile of a field along y (calcYprof, statistics.cu:1943-2003: the
 // average over x and z) is the inverse DFT in y of its kx = kz = 0 modes.
 #pragma once
@@ -17,7 +18,8 @@
 
 namespace gnss {
 
-constexpr int TURB_SUMS = 7;   // e, k^2 e, e/(2|k|), k^2 |s|^2, |w_x|^2, |w_y|^2, |w_z|^2
+constexpr int TURB_SUMS = 4;   // e, k^2 e, e/(2|k|), k^2 |s|^2
+constexpr int VORT_SUMS = 4;   // |w|, w_x^2, w_y^2, w_z^2 over the grid
 
 template <typename T>
 __global__ void __launch_bounds__(STAT_THREADS)
@@ -44,13 +46,6 @@ k_turb_partial(const __grid_constant__ FieldSet<T> st, int has_s, Geom g, double
             const V s = st.p[3][idx];
             acc[3].add(wt * ksq * ((double)s.x * s.x + (double)s.y * s.y));   // calcScalarDissipationKernel_mgpu
         }
-        // i k x u (calcOmega1..3, solver.cu:68-114): magnitudes of k2 w - k3 v, k3 u - k1 w, k1 v - k2 u
-        const double o1r = k2 * cx - k3 * bx, o1i = k2 * cy - k3 * by;
-        const double o2r = k3 * ax - k1 * cx, o2i = k3 * ay - k1 * cy;
-        const double o3r = k1 * bx - k2 * ax, o3i = k1 * by - k2 * ay;
-        acc[4].add(wt * (o1r * o1r + o1i * o1i));
-        acc[5].add(wt * (o2r * o2r + o2i * o2i));
-        acc[6].add(wt * (o3r * o3r + o3i * o3i));
     }
     for (int q = 0; q < TURB_SUMS; ++q) red[q][threadIdx.x] = acc[q].s;
     __syncthreads();
@@ -63,31 +58,36 @@ k_turb_partial(const __grid_constant__ FieldSet<T> st, int has_s, Geom g, double
         for (int q = 0; q < TURB_SUMS; ++q) partial[blockIdx.x * TURB_SUMS + q] = red[q][0];
 }
 
-// Sum of sqrt(w1^2 + w2^2 + w3^2) over the physical points of three padded
-// real fields [nx][ny][2 nz2] (VectorMagnitude + volumeAverage,
-// statistics.cu:2005-2040, 1211-1283); one partial per block in column q0 of
-// `partial` (stride TURB_SUMS).
+// Sums over the physical points of the three padded real vorticity fields
+// [nx][ny][2 nz2]: sqrt(w1^2 + w2^2 + w3^2) (VectorMagnitude + volumeAverage,
+// statistics.cu:2005-2040, 1211-1283) and w1^2, w2^2, w3^2
+// (volumeAverage_rms, :1285-1305); one row of VORT_SUMS partials per block.
 template <typename T>
 __global__ void __launch_bounds__(STAT_THREADS)
-k_absvort_partial(const T *__restrict__ w1, const T *__restrict__ w2, const T *__restrict__ w3, Geom g,
-                  double *__restrict__ partial) {
-    __shared__ double red[STAT_THREADS];
-    Kahan acc;
+k_vort_partial(const T *__restrict__ w1, const T *__restrict__ w2, const T *__restrict__ w3, Geom g,
+               double *__restrict__ partial) {
+    __shared__ double red[VORT_SUMS][STAT_THREADS];
+    Kahan acc[VORT_SUMS];
     const long long npts = (long long)g.nx * g.ny * g.nz;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npts;
          p += (long long)gridDim.x * blockDim.x) {
         const long long line = p / g.nz;
         const long long idx = line * 2 * g.nz2 + (p - line * g.nz);
         const double a = w1[idx], b = w2[idx], c = w3[idx];
-        acc.add(sqrt(a * a + b * b + c * c));
+        acc[0].add(sqrt(a * a + b * b + c * c));
+        acc[1].add(a * a);
+        acc[2].add(b * b);
+        acc[3].add(c * c);
     }
-    red[threadIdx.x] = acc.s;
+    for (int q = 0; q < VORT_SUMS; ++q) red[q][threadIdx.x] = acc[q].s;
     __syncthreads();
     for (int w = STAT_THREADS / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < VORT_SUMS; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) partial[blockIdx.x * TURB_SUMS] = red[0];
+    if (threadIdx.x == 0)
+        for (int q = 0; q < VORT_SUMS; ++q) partial[blockIdx.x * VORT_SUMS + q] = red[q][0];
 }
 
 template <int NS>

@@ -170,7 +170,11 @@ template <typename T, int N> struct Launch {
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
                             cudaStream_t s, int pvariant) {
         if constexpr (N == 256 || N == 512) {
-            if (pvariant == GNSS_VARIANT_REGISTER) {   // register-resident column transforms (on request)
+            // register-resident column transforms: on request, and by default where they measured faster
+            // (FP32 at N = 512: 8.23 against 8.38 ms per 512^3 step; slower at N = 256 and in FP64)
+            const bool reg = pvariant == GNSS_VARIANT_REGISTER ||
+                             (pvariant == GNSS_VARIANT_AUTO && N == 512 && sizeof(T) == 4);
+            if (reg) {
                 using C = PRCfg<T, N>;
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;
                 cudaError_t e = prep_smem(kern, C::SMEM);
@@ -684,21 +688,22 @@ template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields 
     return GNSS_OK;
 }
 
-// calcTurbStats_mgpu (statistics.cu:2039-2156): spectral sums, |omega| through
-// three inverse transforms of the vorticity (scratch fields 1..3; field 0 is
-// the transforms' own scratch), mean profiles from the kx = kz = 0 modes.
+// calcTurbStats_mgpu (statistics.cu:2039-2156): spectral sums; the vorticity
+// statistics over the grid after three inverse transforms of the vorticity
+// (scratch fields 1..3; field 0 is the transforms' own scratch); mean
+// profiles from the kx = kz = 0 modes.
 template <typename T>
 static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *out, double *yprof, cudaStream_t s) {
     const Geom &g = c->g;
-    const size_t nvals = TURB_SUMS + 1 + 5 * (size_t)g.ny;
+    const size_t nvals = TURB_SUMS + VORT_SUMS + 5 * (size_t)g.ny;
     if (!c->turb_part) {
-        if (cudaMalloc(&c->turb_part, sizeof(double) * STAT_BLOCKS * TURB_SUMS) != cudaSuccess ||
+        if (cudaMalloc(&c->turb_part, sizeof(double) * STAT_BLOCKS * std::max(TURB_SUMS, VORT_SUMS)) != cudaSuccess ||
             cudaMalloc(&c->turb_dev, sizeof(double) * nvals) != cudaSuccess ||
             cudaMallocHost(&c->turb_host, sizeof(double) * nvals) != cudaSuccess) {
             cudaGetLastError();
             return fail(c, GNSS_ERR_NOMEM, "cannot allocate statistics buffers");
         }
-        c->owned_bytes += sizeof(double) * (STAT_BLOCKS * TURB_SUMS + nvals);
+        c->owned_bytes += sizeof(double) * (STAT_BLOCKS * std::max(TURB_SUMS, VORT_SUMS) + nvals);
     }
     gnss_status stt = ensure_scratch(c, 4);
     if (stt) return stt;
@@ -720,13 +725,15 @@ static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *o
         if (e) return e;
     }
     c->launches += 3;
-    k_absvort_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(reinterpret_cast<const T *>(o[0]),
-                                                               reinterpret_cast<const T *>(o[1]),
-                                                               reinterpret_cast<const T *>(o[2]), g, c->turb_part);
+    k_vort_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(reinterpret_cast<const T *>(o[0]),
+                                                            reinterpret_cast<const T *>(o[1]),
+                                                            reinterpret_cast<const T *>(o[2]), g, c->turb_part);
     LAUNCH_CK(c);
-    k_sums_final<1><<<1, 32, 0, s>>>(c->turb_part, STAT_BLOCKS, TURB_SUMS, c->turb_dev + TURB_SUMS);
+    k_sums_final<VORT_SUMS><<<1, VORT_SUMS * 32, 0, s>>>(c->turb_part, STAT_BLOCKS, VORT_SUMS,
+                                                         c->turb_dev + TURB_SUMS);
     LAUNCH_CK(c);
-    k_yprof<T><<<5, 256, 0, s>>>(F, g, reinterpret_cast<const V2<T> *>(c->tw[1]), c->turb_dev + TURB_SUMS + 1);
+    k_yprof<T><<<5, 256, 0, s>>>(F, g, reinterpret_cast<const V2<T> *>(c->tw[1]),
+                                 c->turb_dev + TURB_SUMS + VORT_SUMS);
     LAUNCH_CK(c);
     CK(c, cudaMemcpyAsync(c->turb_host, c->turb_dev, sizeof(double) * nvals, cudaMemcpyDeviceToHost, s));
     CK(c, cudaStreamSynchronize(s));
@@ -742,11 +749,11 @@ static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *o
     out->l = 3 * M_PI / 4 * (h[2] / n2) / out->ke;
     out->lambda = std::sqrt(15.0 * nu * out->vrms * out->vrms / out->epsilon);
     out->chi = st->s ? 2.0 * (nu / k.sc) * (h[3] / n2) : 0.0;
-    out->omega_x = std::sqrt(h[4] / n2);
-    out->omega_y = std::sqrt(h[5] / n2);
-    out->omega_z = std::sqrt(h[6] / n2);
     out->omega = h[TURB_SUMS] / nn;
-    if (yprof) std::memcpy(yprof, h + TURB_SUMS + 1, sizeof(double) * 5 * (size_t)g.ny);
+    out->omega_x = std::sqrt(h[TURB_SUMS + 1] / nn);
+    out->omega_y = std::sqrt(h[TURB_SUMS + 2] / nn);
+    out->omega_z = std::sqrt(h[TURB_SUMS + 3] / nn);
+    if (yprof) std::memcpy(yprof, h + TURB_SUMS + VORT_SUMS, sizeof(double) * 5 * (size_t)g.ny);
     return GNSS_OK;
 }
 
@@ -842,6 +849,12 @@ gnss_status gnss_profile_read(gnss_ctx *c, double *ms, long long *launches) {
 }
 
 size_t gnss_field_bytes(const gnss_ctx *ctx) { return ctx ? ctx->nspec * ctx->elem : 0; }
+
+gnss_status gnss_get_config(const gnss_ctx *ctx, gnss_config *out) {
+    if (!ctx || !out) return GNSS_ERR_INVALID;
+    *out = ctx->cfg;
+    return GNSS_OK;
+}
 size_t gnss_workspace_bytes(const gnss_ctx *ctx) { return ctx ? ctx->owned_bytes : 0; }
 
 // scratch fields any operation of this context can ask for (the step's, or one field for the transforms)

@@ -5,9 +5,10 @@
 // kept / compact rows and outer indices, up to two outputs per tile, each the
 // transform of the tile times a spectral multiplier, optional dealias mask),
 // with a different schedule: warp w owns column w of the tile and transforms
-// it in registers with zr_fft (one transpose through its own scratch), so a
-// column crosses shared memory three times (load, transpose, store) and the
-// block synchronises per tile and per output instead of per radix stage.
+// it in registers with zr_fft (one transpose, inside the warp's column of the
+// output tile), so a column crosses shared memory three times (load,
+// transpose, store) and the block synchronises per tile and per output
+// instead of per radix stage.
 //   tile rows are padded to NB + 1 elements: a warp reading one column and a
 //   half-warp pair writing one row are both free of bank conflicts;
 //   the next tile is copied with cp.async (rows the spec does not keep are
@@ -15,7 +16,8 @@
 //   the dealias mask keeps rows whose |index| is at most a bound computed
 //   once per tile and column (k^2 grows with |k_row|), with the reference's
 //   test k^2 > kmax^2 (solver.cu:36) evaluated in the reference's order;
-//   results go through the consumed input buffer to coalesced row stores.
+//   results go through the output tile to coalesced row stores; a second
+//   output of the same tile reloads the input column from shared memory.
 #pragma once
 #include "zreg.cuh"
 
@@ -27,7 +29,20 @@ template <typename T, int N> struct PRCfg {
     static constexpr int NT = NB * 32;
     static constexpr int LD = NB + 1;                     // padded row
     static constexpr int TILE = N * LD;
-    static constexpr int SMEM = (2 * TILE + NB * Z::SCR + Z::LOGE * 32) * (int)sizeof(V2<T>);
+    // two input tiles (the copy pipeline) and one output tile
+    static constexpr int SMEM = (3 * TILE + Z::LOGE * 32) * (int)sizeof(V2<T>);
+};
+
+// zr_fft's transpose inside the warp's own column of the output tile: row k1
+// of the transpose is rows 32 k1 .. 32 k1 + 31 of the column, entry i at
+// i ^ (2 k1) for G = 2 and i ^ (4 k1) for G = 4 (XOR swizzle: with the odd
+// row pitch LD, both the stores and the transposed loads of a warp are free
+// of bank conflicts).
+template <typename T, int N> struct ColScratch {
+    __device__ __forceinline__ int operator()(int k1, int i) const {
+        constexpr int G = ZRCfg<T, N>::G;
+        return (32 * k1 + (i ^ ((G * k1) & 31))) * PRCfg<T, N>::LD;
+    }
 };
 
 // |row index| of a transform row (the Nyquist row counts as N/2)
@@ -43,8 +58,8 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     constexpr int RSTEP = NT / NB;   // rows per copy sweep (32)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tiles = reinterpret_cast<V *>(smem_raw);
-    V *scr_all = tiles + 2 * TILE;
-    V *tws = scr_all + NB * Z::SCR;
+    V *outt = tiles + 2 * TILE;
+    V *tws = outt + TILE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = sp.outer.count() * sp.ncolblk;
     const long long nitems = (long long)sp.nin * ntiles;
@@ -76,18 +91,18 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     };
     prefetch(item, tiles);
     cp_async_commit();
-    V *scr = scr_all + warp * Z::SCR;
     int buf = 0;
+    const int b = warp;   // this warp's column
+    V *col = outt + b;    // this warp's column of the output tile (also its transpose space)
     for (; item < nitems; item += gridDim.x) {
         cp_async_wait<0>();
-        __syncthreads();   // current tile landed; the other buffer's last readers are done
+        __syncthreads();   // current tile landed; the other input tile and the output tile are free
         const long long next = item + gridDim.x;
         if (next < nitems) prefetch(next, tiles + (buf ^ 1) * TILE);
         cp_async_commit();
         int fi, oc, o, c0;
         decode(item, fi, oc, o, c0);
-        V *cur = tiles + buf * TILE;
-        const int b = warp;                       // this warp's column
+        const V *cur = tiles + buf * TILE;
         const bool col_ok = c0 + b < sp.ncols;
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
         const double kc = wavenum(c0 + b, sp.n_col, sp.dk_col);
@@ -102,14 +117,6 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             }
             dmax = cnt - 1;
         }
-        V a[E];
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int row = lane + 32 * m;
-            const bool ok = col_ok && sp.row_in.kept(row) && row_dist<N>(row) <= dmax;
-            a[m] = ok ? cur[row * LD + b] : V{T(0), T(0)};
-        }
-        __syncthreads();   // tile consumed: `cur` becomes the output tile
         const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0;
         const int nv = sp.nvar[fi];
@@ -118,11 +125,13 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             V x[E];
 #pragma unroll
             for (int m = 0; m < E; ++m) {
-                const V q = a[m];
+                const int row = lane + 32 * m;
+                const bool ok = col_ok && sp.row_in.kept(row) && row_dist<N>(row) <= dmax;
+                const V q = ok ? cur[row * LD + b] : V{T(0), T(0)};
                 if (mul == V_ONE) {
                     x[m] = q;
                 } else {
-                    const double kr = wavenum(lane + 32 * m, sp.n_row, sp.dk_row);
+                    const double kr = wavenum(row, sp.n_row, sp.dk_row);
                     if (mul == V_IK_ROW) x[m] = V{(T)(-kr) * q.y, (T)kr * q.x};
                     else if (mul == V_IK_OUT) x[m] = V{(T)(-k_out) * q.y, (T)k_out * q.x};
                     else if (mul == V_IK_COL) x[m] = V{(T)(-kc) * q.y, (T)kc * q.x};
@@ -132,9 +141,9 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                     }
                 }
             }
-            zr_fft<T, N, SIGN>(lane, x, scr, tws);
+            zr_fft<T, N, SIGN>(lane, x, col, tws, ColScratch<T, N>{});
 #pragma unroll
-            for (int q = 0; q < E; ++q) cur[zr_out_index<T, N>(lane, q) * LD + b] = x[q];
+            for (int q = 0; q < E; ++q) col[zr_out_index<T, N>(lane, q) * LD] = x[q];
             __syncthreads();   // output tile complete
             V *dst = P.out[sp.vout[fi][v]] + dbase;
             const int bb = tid % NB;
@@ -143,7 +152,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                 for (int rc = tid / NB; rc < nrow; rc += RSTEP) {
                     const int row = sp.row_out.expand(rc);
                     const int r = sp.row_out_compact ? rc : row;
-                    dst[(long long)r * sp.d_row + bb] = cur[row * LD + bb];
+                    dst[(long long)r * sp.d_row + bb] = outt[row * LD + bb];
                 }
             }
             if (v + 1 < nv) __syncthreads();   // output tile free for the next output

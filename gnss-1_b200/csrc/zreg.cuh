@@ -127,15 +127,22 @@ template <typename V> __device__ __forceinline__ V shfl_xor_v(V v, int m) {
     return V{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
 }
 
+// Transpose layout of zr_fft in a warp's own scratch line: row k1 of 32 + G
+// entries (conflict-free both ways).
+template <typename T, int N> struct ZrScratch {
+    __device__ __forceinline__ int operator()(int k1, int i) const { return k1 * ZRCfg<T, N>::S + i; }
+};
+
 // Length-N DFT of one line held by a warp.  On entry x[m] is element
 // lane + 32 m; on return x[q] is element k1 + E q + E^2 zr_sigma(j) of the
-// transform, with k1 = lane / G, j = lane % G.  scr: this warp's scratch;
+// transform, with k1 = lane / G, j = lane % G.  The one transpose goes
+// through scr at offsets at(k1, i) (row k1 = 0..E-1, entry i = 0..31);
 // tws: table powers tws[32 b + l] = exp(-2 pi i l 2^b / N).
-template <typename T, int N, int SIGN>
-__device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<T> *tws) {
+template <typename T, int N, int SIGN, class AT = ZrScratch<T, N>>
+__device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<T> *tws, AT at = AT{}) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
-    constexpr int E = Z::E, G = Z::G, S = Z::S;
+    constexpr int E = Z::E, G = Z::G;
     Dft<E, SIGN, V>::run(x);
     {
         // W^k1 for k1 = 1, 2, 4 (, 8) from the table, the others as products
@@ -168,11 +175,11 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
         x[7] = cmul(x[7], cmul(w3, w4));
     }
 #pragma unroll
-    for (int k1 = 0; k1 < E; ++k1) scr[k1 * S + lane] = x[k1];
+    for (int k1 = 0; k1 < E; ++k1) scr[at(k1, lane)] = x[k1];
     __syncwarp();
     const int k1 = lane / G, j = lane % G;
 #pragma unroll
-    for (int l = 0; l < E; ++l) x[l] = scr[k1 * S + G * l + j];
+    for (int l = 0; l < E; ++l) x[l] = scr[at(k1, G * l + j)];
     __syncwarp();
     Dft<E, SIGN, V>::run(x);
     zr_tw32_all<SIGN, G, 1, E>(x, j);

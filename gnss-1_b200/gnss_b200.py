@@ -103,6 +103,19 @@ _SIGS = {
     "gnss_get_option": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
     "gnss_scratch_bytes": [_VP],
+    "gnss_get_config": [_VP, ctypes.POINTER(GnssConfig)],
+    "gnss_io_write_field": [ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_char_p],
+    "gnss_io_read_field": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _VP],
+    "gnss_io_write_slice": [ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int,
+                            ctypes.c_char_p],
+    "gnss_io_write_stat": [ctypes.c_char_p, ctypes.c_double, ctypes.c_int],
+    "gnss_io_write_profile": [ctypes.c_int, _VP, ctypes.c_char_p],
+    "gnss_save_state": [_VP, ctypes.POINTER(GnssFields), ctypes.c_char_p, ctypes.c_int, _VP],
+    "gnss_load_state": [_VP, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(GnssFields), _VP],
+    "gnss_checkpoint_save": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields), ctypes.c_longlong,
+                             ctypes.c_char_p, _VP],
+    "gnss_checkpoint_load": [_VP, ctypes.c_char_p, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields),
+                             ctypes.POINTER(ctypes.c_longlong), _VP],
     "gnss_turb_stats": [_VP, ctypes.POINTER(GnssFields), _VP, ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_attach_scratch": [_VP, _VP, ctypes.c_size_t],
     "gnss_ensemble_create": [ctypes.POINTER(GnssConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
@@ -379,6 +392,32 @@ class Context:
         d = {k: getattr(t, k) for k, _ in GnssTurb._fields_}
         d["lambda"] = d.pop("lambda_")
         return d, prof
+
+    # -- files (iofuncs.cu formats, exact checkpoint) -------------------------
+    def save_state(self, state: Sequence, directory, iteration: int, stream=None) -> None:
+        """save3Dfields (iofuncs.cu:360-432): <dir>/u.<iter>, v, w, z, c in physical space."""
+        f = _fields(state)
+        self._ck(self.lib.gnss_save_state(self._h, ctypes.byref(f), str(directory).encode(), int(iteration),
+                                          _stream(stream)), "gnss_save_state")
+
+    def load_state(self, directory, iteration: int, state: Sequence, stream=None) -> None:
+        """importVelocity / importScalar + forward transforms into `state`."""
+        f = _fields(state)
+        self._ck(self.lib.gnss_load_state(self._h, str(directory).encode(), int(iteration), ctypes.byref(f),
+                                          _stream(stream)), "gnss_load_state")
+
+    def checkpoint_save(self, state: Sequence, hist: Sequence | None, step: int, path, stream=None) -> None:
+        f, h = _fields(state), _fields(hist)
+        self._ck(self.lib.gnss_checkpoint_save(self._h, ctypes.byref(f), ctypes.byref(h) if h else None, int(step),
+                                               str(path).encode(), _stream(stream)), "gnss_checkpoint_save")
+
+    def checkpoint_load(self, path, state: Sequence, hist: Sequence | None, stream=None) -> int:
+        f, h = _fields(state), _fields(hist)
+        step = ctypes.c_longlong()
+        self._ck(self.lib.gnss_checkpoint_load(self._h, str(path).encode(), ctypes.byref(f),
+                                               ctypes.byref(h) if h else None, ctypes.byref(step), _stream(stream)),
+                 "gnss_checkpoint_load")
+        return step.value
 
     def set_option(self, key: int, value: int) -> None:
         self._ck(self.lib.gnss_set_option(self._h, key, value), "gnss_set_option")
@@ -677,3 +716,47 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+# ---------------------------------------------------------------------- reference file formats
+GNSS_PLANE_XY, GNSS_PLANE_XZ, GNSS_PLANE_YZ = 0, 1, 2
+
+
+def _io_ck(st: int, what: str) -> None:
+    if st != GNSS_OK:
+        raise GnssError(st, what)
+
+
+def padded_shape(nx: int, ny: int, nz: int) -> tuple:
+    """Shape of a physical field in the reference's in-place layout."""
+    return (nx, ny, 2 * (nz // 2 + 1))
+
+
+def io_write_field(phys: np.ndarray, nz: int, path) -> None:
+    """write3Dfields_mgpu (iofuncs.cu:329-358): phys float64 [nx][ny][2 nz2]."""
+    a = np.ascontiguousarray(phys, dtype=np.float64)
+    _io_ck(load_library().gnss_io_write_field(a.shape[0], a.shape[1], nz, a.ctypes.data, str(path).encode()),
+           "gnss_io_write_field")
+
+
+def io_read_field(nx: int, ny: int, nz: int, path) -> np.ndarray:
+    """loadData (iofuncs.cu:462-497) into a zero-padded array [nx][ny][2 nz2]."""
+    a = np.zeros(padded_shape(nx, ny, nz))
+    _io_ck(load_library().gnss_io_read_field(nx, ny, nz, str(path).encode(), a.ctypes.data), "gnss_io_read_field")
+    return a
+
+
+def io_write_slice(phys: np.ndarray, nz: int, plane: int, index: int, path) -> None:
+    a = np.ascontiguousarray(phys, dtype=np.float64)
+    _io_ck(load_library().gnss_io_write_slice(a.shape[0], a.shape[1], nz, a.ctypes.data, int(plane), int(index),
+                                              str(path).encode()), "gnss_io_write_slice")
+
+
+def io_write_stat(path, value: float, append: bool) -> None:
+    _io_ck(load_library().gnss_io_write_stat(str(path).encode(), float(value), int(bool(append))),
+           "gnss_io_write_stat")
+
+
+def io_write_profile(prof: np.ndarray, path) -> None:
+    a = np.ascontiguousarray(prof, dtype=np.float64)
+    _io_ck(load_library().gnss_io_write_profile(a.size, a.ctypes.data, str(path).encode()), "gnss_io_write_profile")

@@ -90,6 +90,8 @@ typedef struct gnss_ctx gnss_ctx;
 gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out);
 /* Release a context and all memory it owns (cufftDestroy in allocate.cu:297-301). */
 gnss_status gnss_destroy(gnss_ctx *ctx);
+/* The configuration a context was created with. */
+gnss_status gnss_get_config(const gnss_ctx *ctx, gnss_config *out);
 /* Bytes of one field buffer (nx*ny*nz2 complex of the context's precision). */
 size_t gnss_field_bytes(const gnss_ctx *ctx);
 /* Bytes of device memory the context owns right now. */
@@ -165,7 +167,8 @@ gnss_status gnss_stats(gnss_ctx *ctx, const gnss_fields *state, double *out, voi
  *   chi      2 nu/sc sum k^2 |s_hat|^2 / NN^2                    (calcScalarDissipationRate)
  *   omega    volume average of |curl u|                         (:2097-2106)
  *   omega_x, omega_y, omega_z  rms of each vorticity component (:2103-2105)
- * Sums run over the full spectrum (kz mirror) in a fixed order.  yprof (may
+ * Spectral sums run over the full spectrum (kz mirror), the vorticity
+ * statistics over the grid points, both in a fixed order.  yprof (may
  * be NULL) receives 5 x ny doubles: the mean profiles along y (averages over
  * x and z) of u, v, w, s, c (zeros for a missing c) (calcYprof, :1943-2003).
  * Uses four scratch fields of the context; synchronises the stream. */
@@ -216,7 +219,9 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  * transforms):
  *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
  *                          resident line transforms for the z stage where
- *                          they exist (N = 256, 512) and fit, staged passes;
+ *                          they exist (N = 256, 512) and fit; for the passes
+ *                          register transforms in FP32 at N = 512, staged
+ *                          otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
  *                          (N = 256, 512) and fit (a request, not a guarantee);
  *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory.
@@ -319,6 +324,48 @@ gnss_status gnss_server_wait(gnss_server *srv, long long id, double timeout_s);
  * Returns the request's own status (GNSS_ERR_* if it failed). */
 gnss_status gnss_server_result(gnss_server *srv, long long id, void *host_state_out, double *stats, double *times);
 gnss_status gnss_server_report_get(gnss_server *srv, gnss_server_report *out);
+
+/* ---------------------------------------------------------------- files
+ * The reference's file formats (iofuncs.cu) and an exact checkpoint.
+ * Physical fields are host arrays of doubles in the padded in-place layout
+ * [nx][ny][2 (nz/2+1)] of the reference. */
+#define GNSS_PLANE_XY 0   /* fixed z (writexyfields, iofuncs.cu:187-209) */
+#define GNSS_PLANE_XZ 1   /* fixed y (writexzfields, iofuncs.cu:211-233) */
+#define GNSS_PLANE_YZ 2   /* fixed x (writeyzfields, iofuncs.cu:235-257) */
+/* 3D field file: one double holding the byte count 8 nx ny nz, then the
+ * values in [x][y][z] order (write3Dfields_mgpu, iofuncs.cu:329-358). */
+gnss_status gnss_io_write_field(int nx, int ny, int nz, const double *phys, const char *path);
+/* Reads a 3D field file into the padded layout, leaving the padding as it
+ * was (loadData, iofuncs.cu:462-497); GNSS_ERR_INVALID when the byte count
+ * in the file does not match nx ny nz. */
+gnss_status gnss_io_read_field(int nx, int ny, int nz, const char *path, double *phys);
+/* One plane of a 3D field: the byte count as a double, then the values
+ * (x then y for xy; x then z for xz; y then z for yz). */
+gnss_status gnss_io_write_slice(int nx, int ny, int nz, const double *phys, int plane, int index, const char *path);
+/* One statistics record, a raw double; the file is created when append == 0
+ * and appended to otherwise (writeStats, iofuncs.cu:128-146). */
+gnss_status gnss_io_write_stat(const char *path, double value, int append);
+/* A mean profile: ny raw doubles (writeYprofs, iofuncs.cu:78-98). */
+gnss_status gnss_io_write_profile(int ny, const double *prof, const char *path);
+/* A state in the reference's files <dir>/u.<iter>, v, w, z (the scalar s), c
+ * (save3Dfields, iofuncs.cu:360-432).  Each field is transformed to physical
+ * space in a temporary buffer, so the state itself is untouched (the
+ * reference transforms in place and back); FP32 values are widened; c is
+ * written as zeros with one scalar.  Synchronises the stream. */
+gnss_status gnss_save_state(gnss_ctx *ctx, const gnss_fields *state, const char *dir, int iter, void *stream);
+/* Reads such files and forward-transforms them into the state
+ * (importVelocity / importScalar, iofuncs.cu:499-535, then main.cu:149-153).
+ * A missing scalar file leaves that field zero.  Synchronises the stream. */
+gnss_status gnss_load_state(gnss_ctx *ctx, const char *dir, int iter, const gnss_fields *state, void *stream);
+/* Exact checkpoint (no counterpart in the reference, whose restart goes
+ * through physical space): the grid, precision, scalar count, scheme, a step
+ * counter and the spectral state and history bit for bit.  hist may be NULL
+ * (GNSS_SCHEME_RK3IF keeps none); loading checks the file against the
+ * context.  Both synchronise the stream. */
+gnss_status gnss_checkpoint_save(gnss_ctx *ctx, const gnss_fields *state, const gnss_fields *hist, long long step,
+                                 const char *path, void *stream);
+gnss_status gnss_checkpoint_load(gnss_ctx *ctx, const char *path, const gnss_fields *state, const gnss_fields *hist,
+                                 long long *step, void *stream);
 
 /* Forward transform that allocates nothing.  No counterpart in the
  * reference.  For callers that may not allocate device memory: code running

@@ -25,6 +25,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cmath>
+#include <sys/stat.h>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -227,9 +229,60 @@ static int timeit(int argc, char **argv) {
     return 0;
 }
 
+// The reference's file writers (iofuncs.cu:78-260, 329-358), declared here as
+// they are defined there (iofuncs.h declares only some of them).
+void writeYprofs(const int c, const char *name, double *data);
+void writeStats(const int c, const char *name, double in);
+void writexyfields(gpudata gpu, const int iter, const char var, double **in, const int zplane);
+void writexzfields(gpudata gpu, const int iter, const char var, double **in, const int yplane);
+void writeyzfields(gpudata gpu, const int iter, const char var, double **in, const int xplane);
+void write3Dfields_mgpu(gpudata gpu, const int iter, const char var, double **in);
+
+// refdrv io: runs the reference's writers on a synthetic physical field, in
+// the current directory (rootdir "./", sim_name "refdrv/"): refdrv/u.3,
+// refdrv/vis/u_{xy,xz,yz}.3 (planes z = 2, y = 1, x = 4), refdrv/stats/KE
+// (three records), refdrv/Yprofs/u_mean.3; the input goes to refdrv/input.bin
+// (the padded array [NX][NY][2 NZ2], padding -1) and refdrv/prof.bin.  Host
+// code only: no CUDA call is made.
+static int io_mode() {
+    const size_t n = (size_t)NX * NY * 2 * NZ2;
+    std::vector<double> f(n, -1.0);
+    for (int i = 0; i < NX; ++i)
+        for (int j = 0; j < NY; ++j)
+            for (int k = 0; k < NZ; ++k)
+                f[k + 2 * NZ2 * (j + NY * (size_t)i)] = i + 0.01 * j + 1e-4 * k + 0.5 * std::sin(0.3 * i + 0.7 * j + 1.1 * k);
+    std::vector<double> prof(NY);
+    for (int j = 0; j < NY; ++j) prof[j] = 0.25 * j - 1.0 / (j + 1);
+    int nx[1] = {NX};
+    gpudata g{};
+    g.nGPUs = 1;
+    g.nx = nx;
+    double *in[1] = {f.data()};
+    mkdir("refdrv", 0700);
+    mkdir("refdrv/vis", 0700);
+    mkdir("refdrv/stats", 0700);
+    mkdir("refdrv/Yprofs", 0700);
+    write3Dfields_mgpu(g, 3, 'u', in);
+    writexyfields(g, 3, 'u', in, 2);
+    writexzfields(g, 3, 'u', in, 1);
+    writeyzfields(g, 3, 'u', in, 4);
+    writeStats(0, "KE", 1.5);
+    writeStats(1, "KE", 2.5);
+    writeStats(2, "KE", -0.125);
+    writeYprofs(3, "u_mean", prof.data());
+    FILE *fp = std::fopen("refdrv/input.bin", "wb");
+    std::fwrite(f.data(), sizeof(double), n, fp);
+    std::fclose(fp);
+    fp = std::fopen("refdrv/prof.bin", "wb");
+    std::fwrite(prof.data(), sizeof(double), NY, fp);
+    std::fclose(fp);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc >= 2 && std::strcmp(argv[1], "run") == 0) return run(argc, argv);
     if (argc >= 2 && std::strcmp(argv[1], "time") == 0) return timeit(argc, argv);
-    std::fprintf(stderr, "usage: refdrv run|time ...\n");
+    if (argc >= 2 && std::strcmp(argv[1], "io") == 0) return io_mode();
+    std::fprintf(stderr, "usage: refdrv run|time|io ...\n");
     return 1;
 }
