@@ -15,7 +15,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-SOURCES = [HERE / "csrc" / "gnss_b200.cu", HERE / "csrc" / "batch.cpp", HERE / "csrc" / "io.cpp"]
+SOURCES = [HERE / "csrc" / "gnss_b200.cu", HERE / "csrc" / "batch.cpp", HERE / "csrc" / "io.cpp",
+           HERE / "csrc" / "ic.cu"]
 DEPS = sorted((HERE / "csrc").glob("*")) + [ROOT / "include" / "gnss_b200.h"]
 OUT = HERE / "libgnss_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

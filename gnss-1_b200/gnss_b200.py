@@ -64,6 +64,11 @@ class GnssTurb(ctypes.Structure):
                                                "omega_x", "omega_y", "omega_z")]
 
 
+class GnssJetParams(ctypes.Structure):
+    _fields_ = [("h", ctypes.c_double), ("theta", ctypes.c_double), ("theta_c", ctypes.c_double),
+                ("pert_amp", ctypes.c_double), ("seed", ctypes.c_uint)]
+
+
 class GnssFields(ctypes.Structure):
     _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p),
                 ("s", ctypes.c_void_p), ("c", ctypes.c_void_p)]
@@ -103,6 +108,7 @@ _SIGS = {
     "gnss_get_option": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
     "gnss_profile_read": [_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)],
     "gnss_scratch_bytes": [_VP],
+    "gnss_initial_jet": [_VP, ctypes.POINTER(GnssJetParams), ctypes.POINTER(GnssFields), _VP],
     "gnss_get_config": [_VP, ctypes.POINTER(GnssConfig)],
     "gnss_io_write_field": [ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_char_p],
     "gnss_io_read_field": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _VP],
@@ -392,6 +398,14 @@ class Context:
         d = {k: getattr(t, k) for k, _ in GnssTurb._fields_}
         d["lambda"] = d.pop("lambda_")
         return d, prof
+
+    def initial_jet(self, state: Sequence, h: float = 1.0, theta: float = 0.05, theta_c: float = 0.05,
+                    pert_amp: float = 0.05, seed: int = 0, stream=None) -> None:
+        """The reference's initializeJet (initialize.cu:615-641) + forward transforms + dealias (main.cu:149-156)."""
+        p = GnssJetParams(h, theta, theta_c, pert_amp, seed)
+        f = _fields(state)
+        self._ck(self.lib.gnss_initial_jet(self._h, ctypes.byref(p), ctypes.byref(f), _stream(stream)),
+                 "gnss_initial_jet")
 
     # -- files (iofuncs.cu formats, exact checkpoint) -------------------------
     def save_state(self, state: Sequence, directory, iteration: int, stream=None) -> None:

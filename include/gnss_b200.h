@@ -367,6 +367,25 @@ gnss_status gnss_checkpoint_save(gnss_ctx *ctx, const gnss_fields *state, const 
 gnss_status gnss_checkpoint_load(gnss_ctx *ctx, const char *path, const gnss_fields *state, const gnss_fields *hist,
                                  long long *step, void *stream);
 
+/* The reference's initial temporal jet (initializeJet, initialize.cu:615-641)
+ * followed by forward transforms and dealiasing (main.cu:149-156), written
+ * into the spectral state.  u = 0.5 - 0.5 tanh(h/(4 theta)(2|y|/h - 1)) plus
+ * pert_amp times solenoidal noise with the reference's Gaussian spectrum
+ * (generateNoise, initialize.cu:303-612), v and w the noise alone, s the same
+ * profile with theta, c with theta_c; y = -ly/2 + j ly/ny.  The noise draws
+ * come from the C library's rand() generator seeded with
+ * srand(666*37 + 37*13) as in the reference (seed 0), or with `seed`,
+ * through a private state, in the reference's loop order on the host; the
+ * transforms and profiles run on the device.  Synchronises the stream. */
+typedef struct gnss_jet_params {
+    double h;          /* jet width H (dnsparams.h)                         */
+    double theta;      /* momentum thickness of u and s (theta)             */
+    double theta_c;    /* thickness of the c profile (theta_c)              */
+    double pert_amp;   /* noise amplitude (pert_amp)                        */
+    unsigned seed;     /* 0: the reference's seed                           */
+} gnss_jet_params;
+gnss_status gnss_initial_jet(gnss_ctx *ctx, const gnss_jet_params *p, const gnss_fields *state, void *stream);
+
 /* Forward transform that allocates nothing.  No counterpart in the
  * reference.  For callers that may not allocate device memory: code running
  * under a memory manager that owns the whole device (a framework's caching

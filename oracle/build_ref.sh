@@ -29,21 +29,23 @@ if [ ! -f "$REF/solver.cu" ]; then
     exit 1
 fi
 
-# name  N    Re      Sc   Sc_c  alpha  dt
+# name  N    Re      Sc   Sc_c  alpha  dt      pert_amp (noise of the initial jet, initialize.cu:615-641)
 CONFIGS="
-g12    12   200.0   0.7  1.0   0.0    2.0e-3
-g16    16   200.0   0.7  1.0   0.0    2.0e-3
-g16a   16   200.0   0.7  1.0   0.05   2.0e-3
-c64    64   1000.0  0.7  0.7   0.0    1.0e-3
-c128   128  1000.0  0.7  0.7   0.0    1.0e-3
-c256   256  3000.0  0.7  1.0   0.0    5.0e-4
-c512   512  5000.0  0.7  0.7   0.0    2.5e-4
+g12    12   200.0   0.7  1.0   0.0    2.0e-3  0.0
+g16    16   200.0   0.7  1.0   0.0    2.0e-3  0.0
+g16a   16   200.0   0.7  1.0   0.05   2.0e-3  0.0
+i16    16   200.0   0.7  1.0   0.0    2.0e-3  0.05
+i32    32   1000.0  0.7  1.0   0.0    1.0e-3  0.05
+c64    64   1000.0  0.7  0.7   0.0    1.0e-3  0.0
+c128   128  1000.0  0.7  0.7   0.0    1.0e-3  0.0
+c256   256  3000.0  0.7  1.0   0.0    5.0e-4  0.0
+c512   512  5000.0  0.7  0.7   0.0    2.5e-4  0.0
 "
 
 want=("$@")
 SRCS=(solver cudafuncs fftfuncs allocate initialize iofuncs statistics)
 
-gen_params() {  # N Re Sc Sc_c alpha dt
+gen_params() {  # N Re Sc Sc_c alpha dt pert_amp
     cat <<EOF
 /* generated by oracle/build_ref.sh: the temporal-jet configuration of the
  * reference (dnsparams.h:9-41) with runtime sizes fixed for this build */
@@ -75,7 +77,7 @@ gen_params() {  # N Re Sc Sc_c alpha dt
 #define Sc_c $4
 #define alpha $5
 #define alias_filter (2.0/3.0)
-#define pert_amp 0.0
+#define pert_amp $7
 #define rootdir "./"
 #define sim_name "refdrv/"
 #define RAD 1
@@ -83,7 +85,7 @@ EOF
 }
 
 build_one() {
-    local name=$1 n=$2 re=$3 sc=$4 scc=$5 al=$6 dtv=$7
+    local name=$1 n=$2 re=$3 sc=$4 scc=$5 al=$6 dtv=$7 pert=$8
     local d="$OUT/$name"
     mkdir -p "$d/src" "$d/obj"
     for f in "$REF"/*.cu "$REF"/*.h; do
@@ -91,7 +93,7 @@ build_one() {
         [ "$b" = "dnsparams.h" ] && continue
         ln -sf "$f" "$d/src/$b"
     done
-    gen_params "$n" "$re" "$sc" "$scc" "$al" "$dtv" > "$d/src/dnsparams.h"
+    gen_params "$n" "$re" "$sc" "$scc" "$al" "$dtv" "$pert" > "$d/src/dnsparams.h"
     local objs=()
     for s in "${SRCS[@]}"; do
         # the reference is C++03 code (Makefile:2); C99 "complex double" needs it
@@ -118,14 +120,14 @@ build_one() {
 }
 
 pids=()
-while read -r name n re sc scc al dtv; do
+while read -r name n re sc scc al dtv pert; do
     [ -z "${name:-}" ] && continue
     if [ ${#want[@]} -gt 0 ]; then
         keep=0
         for w in "${want[@]}"; do [ "$w" = "$name" ] && keep=1; done
         [ $keep -eq 0 ] && continue
     fi
-    build_one "$name" "$n" "$re" "$sc" "$scc" "$al" "$dtv" &
+    build_one "$name" "$n" "$re" "$sc" "$scc" "$al" "$dtv" "$pert" &
     pids+=($!)
 done <<< "$CONFIGS"
 rc=0

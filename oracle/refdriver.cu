@@ -41,6 +41,15 @@
 #include "solver.h"
 #include "initialize.h"
 
+// generateNoise (initialize.cu:388-390) takes its work arrays from malloc and
+// assigns only the modes with |k| < kmax; the rest (the Nyquist planes among
+// them) is read uninitialized, so its initial condition depends on whatever
+// the heap held (NaN in practice when the arrays come from reused heap
+// memory).  The driver zero-fills every heap allocation of the program, which
+// makes those modes zero, as they are when the arrays come from fresh pages.
+extern "C" void *__libc_calloc(size_t, size_t) noexcept;
+extern "C" void *malloc(size_t n) noexcept { return __libc_calloc(1, n); }
+
 #define DRV_CHECK(x)                                                                        \
     do {                                                                                    \
         cudaError_t e_ = (x);                                                               \
@@ -279,10 +288,30 @@ static int io_mode() {
     return 0;
 }
 
+// refdrv ic <out_dir>: the reference's initial condition as main.cu builds it
+// (initializeJet, main.cu:139; forward transforms, :149-153; deAlias, :156),
+// dumped as <out_dir>/ic.bin (the 5 spectral fields).
+static int ic_mode(int argc, char **argv) {
+    if (argc < 3) { std::fprintf(stderr, "usage: refdrv ic <out_dir>\n"); return 1; }
+    std::string out = argv[2];
+    setup();
+    initializeJet(fft, gpu, grid, h_vel, vel, rhs);
+    forwardTransform(fft, gpu, vel.u);
+    forwardTransform(fft, gpu, vel.v);
+    forwardTransform(fft, gpu, vel.w);
+    forwardTransform(fft, gpu, vel.s);
+    forwardTransform(fft, gpu, vel.c);
+    deAlias(gpu, grid, vel);
+    DRV_CHECK(cudaDeviceSynchronize());
+    dump(out + "/ic.bin", vel);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc >= 2 && std::strcmp(argv[1], "run") == 0) return run(argc, argv);
+    if (argc >= 2 && std::strcmp(argv[1], "ic") == 0) return ic_mode(argc, argv);
     if (argc >= 2 && std::strcmp(argv[1], "time") == 0) return timeit(argc, argv);
     if (argc >= 2 && std::strcmp(argv[1], "io") == 0) return io_mode();
-    std::fprintf(stderr, "usage: refdrv run|time|io ...\n");
+    std::fprintf(stderr, "usage: refdrv run|time|io|ic ...\n");
     return 1;
 }
