@@ -171,9 +171,8 @@ template <typename T, int N> struct Launch {
                             cudaStream_t s, int pvariant) {
         if constexpr (N == 256 || N == 512) {
             // register-resident column transforms: on request, and by default where they measured faster
-            // (FP32 at N = 512: 8.23 against 8.38 ms per 512^3 step; slower at N = 256 and in FP64)
-            const bool reg = pvariant == GNSS_VARIANT_REGISTER ||
-                             (pvariant == GNSS_VARIANT_AUTO && N == 512 && sizeof(T) == 4);
+            // (N = 512: 7.34 against 8.39 ms per 512^3 FP32 step, 10.1 against 8.9 Gpoint-steps/s in FP64)
+            const bool reg = pvariant == GNSS_VARIANT_REGISTER || (pvariant == GNSS_VARIANT_AUTO && N == 512);
             if (reg) {
                 using C = PRCfg<T, N>;
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;

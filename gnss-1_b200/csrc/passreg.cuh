@@ -17,7 +17,10 @@
 //   once per tile and column (k^2 grows with |k_row|), with the reference's
 //   test k^2 > kmax^2 (solver.cu:36) evaluated in the reference's order;
 //   results go through the output tile to coalesced row stores; a second
-//   output of the same tile reloads the input column from shared memory.
+//   output of the same tile reloads the input column from shared memory;
+//   per-element bookkeeping is kept out of the element loops (a per-lane
+//   mask of the rows it loads, the multiplier chosen once per output,
+//   32-bit store offsets).
 #pragma once
 #include "zreg.cuh"
 
@@ -94,6 +97,10 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     int buf = 0;
     const int b = warp;   // this warp's column
     V *col = outt + b;    // this warp's column of the output tile (also its transpose space)
+    // rows lane + 32 m this lane loads: bit m set when the spec keeps the row (fixed for the launch)
+    unsigned keptm = 0;
+#pragma unroll
+    for (int m = 0; m < E; ++m) keptm |= (sp.row_in.kept(lane + 32 * m) ? 1u : 0u) << m;
     for (; item < nitems; item += gridDim.x) {
         cp_async_wait<0>();
         __syncthreads();   // current tile landed; the other input tile and the output tile are free
@@ -107,7 +114,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
         const double kc = wavenum(c0 + b, sp.n_col, sp.dk_col);
         // rows kept by the dealias mask: |row index| <= dmax (prefix by monotonicity of k^2)
-        int dmax = N;
+        unsigned okm = col_ok ? keptm : 0u;
         if (sp.mask) {
             int cnt = 0;
             for (int d0 = 0; d0 <= N / 2; d0 += 32) {
@@ -115,7 +122,10 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                 const bool ok = d <= N / 2 && !(ksq3(sp.dk_row * (double)d, k_out, kc) > sp.kmax2);
                 cnt += __popc(__ballot_sync(0xffffffffu, ok));
             }
-            dmax = cnt - 1;
+            const int dmax = cnt - 1;
+#pragma unroll
+            for (int m = 0; m < E; ++m)
+                if (row_dist<N>(lane + 32 * m) > dmax) okm &= ~(1u << m);
         }
         const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0;
@@ -124,35 +134,37 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             const int mul = sp.vmul[fi][v];
             V x[E];
 #pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const int row = lane + 32 * m;
-                const bool ok = col_ok && sp.row_in.kept(row) && row_dist<N>(row) <= dmax;
-                const V q = ok ? cur[row * LD + b] : V{T(0), T(0)};
-                if (mul == V_ONE) {
-                    x[m] = q;
-                } else {
-                    const double kr = wavenum(row, sp.n_row, sp.dk_row);
-                    if (mul == V_IK_ROW) x[m] = V{(T)(-kr) * q.y, (T)kr * q.x};
-                    else if (mul == V_IK_OUT) x[m] = V{(T)(-k_out) * q.y, (T)k_out * q.x};
-                    else if (mul == V_IK_COL) x[m] = V{(T)(-kc) * q.y, (T)kc * q.x};
-                    else {   // V_LAP
-                        const T k2 = (T)ksq3(kr, k_out, kc);
-                        x[m] = V{-k2 * q.x, -k2 * q.y};
-                    }
+            for (int m = 0; m < E; ++m) x[m] = ((okm >> m) & 1u) ? cur[(lane + 32 * m) * LD + b] : V{T(0), T(0)};
+            if (mul == V_IK_ROW) {
+#pragma unroll
+                for (int m = 0; m < E; ++m) {
+                    const T kr = (T)wavenum(lane + 32 * m, sp.n_row, sp.dk_row);
+                    x[m] = V{-kr * x[m].y, kr * x[m].x};
+                }
+            } else if (mul == V_IK_OUT || mul == V_IK_COL) {
+                const T kk = (T)(mul == V_IK_OUT ? k_out : kc);
+#pragma unroll
+                for (int m = 0; m < E; ++m) x[m] = V{-kk * x[m].y, kk * x[m].x};
+            } else if (mul == V_LAP) {
+#pragma unroll
+                for (int m = 0; m < E; ++m) {
+                    const T k2 = (T)ksq3(wavenum(lane + 32 * m, sp.n_row, sp.dk_row), k_out, kc);
+                    x[m] = V{-k2 * x[m].x, -k2 * x[m].y};
                 }
             }
             zr_fft<T, N, SIGN>(lane, x, col, tws, ColScratch<T, N>{});
 #pragma unroll
             for (int q = 0; q < E; ++q) col[zr_out_index<T, N>(lane, q) * LD] = x[q];
             __syncthreads();   // output tile complete
-            V *dst = P.out[sp.vout[fi][v]] + dbase;
-            const int bb = tid % NB;
-            if (bb < out_cols) {
+            V *dst = P.out[sp.vout[fi][v]] + dbase + tid % NB;
+            if (tid % NB < out_cols) {
                 const int nrow = sp.row_out.count();
+                const int drow = (int)sp.d_row;   // row pitch of the destination (< 2^31 elements per tile)
+                const V *src = outt + tid % NB;
                 for (int rc = tid / NB; rc < nrow; rc += RSTEP) {
                     const int row = sp.row_out.expand(rc);
                     const int r = sp.row_out_compact ? rc : row;
-                    dst[(long long)r * sp.d_row + bb] = outt[row * LD + bb];
+                    dst[r * drow] = src[row * LD];
                 }
             }
             if (v + 1 < nv) __syncthreads();   // output tile free for the next output

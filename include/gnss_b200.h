@@ -220,8 +220,7 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
  *                          resident line transforms for the z stage where
  *                          they exist (N = 256, 512) and fit; for the passes
- *                          register transforms in FP32 at N = 512, staged
- *                          otherwise;
+ *                          register transforms at N = 512, staged otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
  *                          (N = 256, 512) and fit (a request, not a guarantee);
  *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory.
