@@ -170,9 +170,9 @@ template <typename T, int N> struct Launch {
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
                             cudaStream_t s, int pvariant) {
         if constexpr (N == 256 || N == 512) {
-            // register-resident column transforms: on request, and by default where they measured faster
-            // (N = 512: 7.34 against 8.39 ms per 512^3 FP32 step, 10.1 against 8.9 Gpoint-steps/s in FP64)
-            const bool reg = pvariant == GNSS_VARIANT_REGISTER || (pvariant == GNSS_VARIANT_AUTO && N == 512);
+            // register-resident column transforms unless staged ones are requested; measured faster
+            // (512^3 FP32 step 7.34 against 8.39 ms, FP64 10.1 against 8.9 Gpoint-steps/s; 256^3 1.23 against 1.28 ms)
+            const bool reg = pvariant != GNSS_VARIANT_STAGED;
             if (reg) {
                 using C = PRCfg<T, N>;
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;

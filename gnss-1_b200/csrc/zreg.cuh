@@ -97,8 +97,9 @@ template <typename T, int N> struct ZRCfg {
     __host__ __device__ static constexpr int pidx(int n) { return n + PADP * (n >> 6); }
     static_assert(E == 8 || E == 16, "register z transform serves N = 256 and 512");
     static_assert(SCR >= PL, "scratch holds a padded line");
+    // twiddle powers, physical lines, scratch lines, raw staging, mbarrier (16 B), kz table (ncp T)
     __host__ __device__ static constexpr int smem_bytes(int nph, int nraw, int ncp) {
-        return (LOGE * 32 + nph * PL + nph * SCR + nraw * 2 * ncp) * (int)sizeof(V2<T>) + 16;
+        return (LOGE * 32 + nph * PL + nph * SCR + nraw * 2 * ncp) * (int)sizeof(V2<T>) + 16 + ncp * (int)sizeof(T);
     }
 };
 
@@ -209,20 +210,22 @@ template <typename T, int N> __device__ __forceinline__ int zr_out_index(int lan
 }
 
 // C2R packing (as pack_c2r_combo) straight into the registers of zr_fft:
-// x[m] = Z_n, n = lane + 32 m.
+// x[m] = Z_n, n = lane + 32 m.  keep: bit m set when mode min(n, N - n) is a
+// kept kz mode (< nkz); tkz: kz wavenumbers (T) of the kept modes.
 template <typename T, int N>
 __device__ __forceinline__ void zr_pack(int lane, V2<T> *x, const ZRecipe rc, const V2<T> *a0, const V2<T> *a1,
-                                        int ncp, int nkz, double dkz) {
+                                        int ncp, unsigned keep, const T *tkz) {
     using V = V2<T>;
     constexpr int E = ZRCfg<T, N>::E;
+    const bool any_kz = rc.ikz[0] || (a1 && rc.ikz[1]);
 #pragma unroll
     for (int m = 0; m < E; ++m) {
         const int n = lane + 32 * m;
         const bool lo = 2 * n <= N;
         const int k = lo ? n : N - n;
         V z = V{T(0), T(0)};
-        if (k < nkz) {
-            const T kz = (T)wavenum(k, N, dkz);
+        if ((keep >> m) & 1u) {
+            const T kz = any_kz ? tkz[k] : T(0);
             V a = a0[k], b = a0[ncp + k];
             if (rc.ikz[0]) { a = V{-kz * a.y, kz * a.x}; b = V{-kz * b.y, kz * b.x}; }
             if (rc.sgn[0] < 0) { a = V{-a.x, -a.y}; b = V{-b.x, -b.y}; }
@@ -297,10 +300,18 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
     V *scr_all = phys + NPH * PL;
     V *raw = scr_all + NPH * SCR;
     uint64_t *bar = reinterpret_cast<uint64_t *>(raw + NRAW * rawf);
+    T *tkz = reinterpret_cast<T *>(bar + 2);   // kz wavenumbers of the kept modes (ncp entries)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     long long pair = blockIdx.x;
     if (pair >= npairs) return;   // uniform for the block
     for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    for (int k = threadIdx.x; k < ncp; k += blockDim.x) tkz[k] = (T)wavenum(k, N, dkz);
+    unsigned keep = 0;   // bit m: mode min(n, N - n) of element n = lane + 32 m is kept
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int n = (threadIdx.x & 31) + 32 * m;
+        keep |= ((2 * n <= N ? n : N - n) < nkz ? 1u : 0u) << m;
+    }
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         mbar_fence_init();
@@ -324,8 +335,8 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
         }
         parity ^= 1u;
         V x[E];
-        zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp, nkz,
-                      dkz);
+        zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp, keep,
+                      tkz);
         __syncthreads();   // staging consumed; the previous pair's products are read
         if (threadIdx.x == 0 && pair + gridDim.x < npairs) {
             fence_proxy_async_smem();

@@ -218,9 +218,8 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  * the kernel of the strided x and y passes (of the step and of the 3D
  * transforms):
  *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
- *                          resident line transforms for the z stage where
- *                          they exist (N = 256, 512) and fit; for the passes
- *                          register transforms at N = 512, staged otherwise;
+ *                          resident line transforms where they exist
+ *                          (N = 256, 512) and fit, staged otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
  *                          (N = 256, 512) and fit (a request, not a guarantee);
  *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory.
