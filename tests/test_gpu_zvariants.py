@@ -16,13 +16,19 @@ import pytest
 from _util import rel_l2, to_dev, to_host
 
 CASES = [
-    # n, precision, n_scalars, alpha
+    # grid, precision, n_scalars, alpha
     (256, 0, 1, 0.0),
     (256, 0, 2, 0.05),
     (256, 1, 1, 0.0),
     (256, 1, 2, 0.0),
     (512, 1, 1, 0.0),
+    ((64, 64, 512), 0, 2, 0.05),   # z length 512: forward transforms split in halves, 5 products
+    ((64, 64, 512), 1, 1, 0.0),
 ]
+
+
+def _shape(n):
+    return (n, n, n) if isinstance(n, int) else n
 
 
 def _run(G, torch, ctx, init, steps, variant, pvariant=0):
@@ -40,16 +46,18 @@ def _run(G, torch, ctx, init, steps, variant, pvariant=0):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n,precision,ns,alpha", CASES,
-                         ids=[f"n{c[0]}_{'fp64' if c[1] == 0 else 'fp32'}_s{c[2]}{'_alpha' if c[3] else ''}"
-                              for c in CASES])
+                         ids=[f"n{'x'.join(map(str, _shape(c[0])))}_{'fp64' if c[1] == 0 else 'fp32'}_s{c[2]}"
+                              f"{'_alpha' if c[3] else ''}" for c in CASES])
 def test_register_and_staged_z_agree(torch_cuda, n, precision, ns, alpha):
     import gnss_b200 as G
     torch = torch_cuda
+    nx, ny, nz = _shape(n)
     cdt = np.complex128 if precision == 0 else np.complex64
-    init = G.jet_initial_state(n, n_scalars=ns, seed=5, noise_kmax=8.0, amp=0.05, dtype=cdt)
+    init = G.jet_initial_state(nx, ny, nz, n_scalars=ns, seed=5, noise_kmax=8.0, amp=0.05, dtype=cdt)
     tol = 1e-13 if precision == 0 else 2e-6
     A, S = G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED
-    with G.Context(n, re=3000.0, sc=0.7, sc_c=1.0, alpha=alpha, dt=5e-4, n_scalars=ns, precision=precision) as ctx:
+    with G.Context(nx=nx, ny=ny, nz=nz, re=3000.0, sc=0.7, sc_c=1.0, alpha=alpha, dt=5e-4, n_scalars=ns,
+                   precision=precision) as ctx:
         a = _run(G, torch, ctx, init, 2, A, A)
         for zv, pv in ((S, A), (A, S), (S, S)):
             b = _run(G, torch, ctx, init, 2, zv, pv)
