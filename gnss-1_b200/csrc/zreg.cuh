@@ -108,13 +108,20 @@ template <int G> __device__ __forceinline__ int zr_sigma(int j) {
     return G == 2 ? j : ((j >> 1) | ((j & 1) << 1));
 }
 
+// v * W_32^(j Q): lane group member j multiplies, the others keep v
 template <int S, int Q, int G, typename V> __device__ __forceinline__ V zr_tw32(V v, int j) {
+    using T = decltype(v.x);
     if constexpr (G == 2) {
-        const V y = mul_w32<S, Q>(v);
-        return j ? y : v;
+        if (j) v = mul_w32<S, Q>(v);
+        return v;
     } else {
-        const V y1 = mul_w32<S, Q>(v), y2 = mul_w32<S, 2 * Q>(v), y3 = mul_w32<S, 3 * Q>(v);
-        return j == 0 ? v : j == 1 ? y1 : j == 2 ? y2 : y3;
+        constexpr T c1 = (T)cos32(Q), s1 = (T)((double)S * sin32(Q));
+        constexpr T c2 = (T)cos32(2 * Q), s2 = (T)((double)S * sin32(2 * Q));
+        constexpr T c3 = (T)cos32(3 * Q), s3 = (T)((double)S * sin32(3 * Q));
+        if (j == 0) return v;
+        const T c = j == 1 ? c1 : j == 2 ? c2 : c3;
+        const T s = j == 1 ? s1 : j == 2 ? s2 : s3;
+        return V{v.x * c - v.y * s, v.x * s + v.y * c};
     }
 }
 template <int S, int G, int Q, int E, typename V> __device__ __forceinline__ void zr_tw32_all(V *x, int j) {
@@ -184,21 +191,25 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
     __syncwarp();
     Dft<E, SIGN, V>::run(x);
     zr_tw32_all<SIGN, G, 1, E>(x, j);
+    // G-point DFT across the group: each radix-2 step is p + s x with s = +1 on
+    // the lower and -1 on the upper member (p the partner's value)
     if constexpr (G == 2) {
+        const T sg = j == 0 ? T(1) : T(-1);
 #pragma unroll
         for (int q = 0; q < E; ++q) {
             const V p = shfl_xor_v(x[q], 1);
-            x[q] = j == 0 ? cadd(x[q], p) : csub(p, x[q]);
+            x[q] = V{p.x + sg * x[q].x, p.y + sg * x[q].y};
         }
     } else {
         const int j0 = j & 1, j1 = j >> 1;
+        const T s1 = j1 == 0 ? T(1) : T(-1), s0 = j0 == 0 ? T(1) : T(-1);
 #pragma unroll
         for (int q = 0; q < E; ++q) {
             const V p = shfl_xor_v(x[q], 2);
-            V c = j1 == 0 ? cadd(x[q], p) : csub(p, x[q]);
+            V c = V{p.x + s1 * x[q].x, p.y + s1 * x[q].y};
             if (j0 && j1) c = mul_si<SIGN>(c);
             const V p2 = shfl_xor_v(c, 1);
-            x[q] = j0 == 0 ? cadd(c, p2) : csub(p2, c);
+            x[q] = V{p2.x + s0 * c.x, p2.y + s0 * c.y};
         }
     }
 }
