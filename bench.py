@@ -202,11 +202,11 @@ def run_e2e(G, torch, n, precision, scheme, calls, dev):
     e1.record(stream)
     torch.cuda.synchronize(dev)
     ms_call = e0.elapsed_time(e1) / calls
-    state_bytes = host_in.numel() * host_in.element_size()
+    h2d, d2h = ctx.run_host_bytes()    # the kept box of each field in, the whole state out
     ctx.close()
     del host_in, host_out
-    return dict(ms_call=ms_call, h2d=state_bytes / E2E_STEPS_PER_CALL,
-                d2h=(state_bytes + E2E_STEPS_PER_CALL * G.GNSS_NSTATS * 8) / E2E_STEPS_PER_CALL)
+    return dict(ms_call=ms_call, h2d=h2d / E2E_STEPS_PER_CALL,
+                d2h=(d2h + E2E_STEPS_PER_CALL * 6 * 8) / E2E_STEPS_PER_CALL)   # + six double sums per step
 
 
 def run_error_vs_fp64(G, torch, n, steps, dev) -> dict:

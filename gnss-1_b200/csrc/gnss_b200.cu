@@ -35,6 +35,11 @@ struct gnss_ctx {
     double *turb_dev = nullptr;                   // TURB_SUMS + 1 sums, then 5 * ny profile values
     double *turb_host = nullptr;                  // pinned copy of turb_dev
     void *res = nullptr;                          // resident state + history for gnss_run_host (2 * nf fields)
+    double *run_sums = nullptr;                   // gnss_run_host: STAT_SUMS per step, summed by the update
+    double *run_sums_host = nullptr;              // pinned copy of run_sums
+    int run_sums_cap = 0;                         // steps run_sums holds
+    cudaStream_t side = nullptr;                  // gnss_run_host: download of the modes outside the kept box
+    cudaEvent_t side_ev[2] = {nullptr, nullptr};  // state ready / side copies done
     size_t owned_bytes = 0;
     // fused step layout (set_recipes): x-inverse outputs P, y-inverse outputs
     // (the raw quantities of the z pass) Q, physical quantities, products
@@ -537,7 +542,7 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
 //   6 projection, dealias and time update                                  (P, state, hist)
 template <typename T>
 static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, void *hist_base, const gnss_fields *hist,
-                                        const UpdCoef &uc, cudaStream_t s) {
+                                        const UpdCoef &uc, cudaStream_t s, double *stats_dst = nullptr) {
     const Geom &g = c->g;
     const int np = c->n_xout, nq = c->n_raw, nnl = c->nnl;
     gnss_status st = ensure_scratch_step(c);
@@ -606,7 +611,21 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
         // one warp per kept (ky, kx) row; 8 blocks of 8 warps per SM
         const long long nrows = (long long)c->ky_keep.count() * c->kx_keep.count();
         const int full_rows = (uc.scheme == GNSS_SCHEME_CNAB2 && uc.euler) ? 1 : 0;
-        const long long nblk = std::min<long long>((nrows + 7) / 8, 8LL * c->nsm);
+        long long nblk = std::min<long long>((nrows + 7) / 8, 8LL * c->nsm);
+        if (stats_dst) {   // statistics of the new state summed by the update itself (one partial row per block)
+            nblk = std::min<long long>(nblk, STAT_BLOCKS);
+            if (uc.scheme == GNSS_SCHEME_CNAB2)
+                k_update<T, GNSS_SCHEME_CNAB2, true><<<(unsigned)nblk, 256, 0, s>>>(
+                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, c->stat_part);
+            else
+                k_update<T, GNSS_SCHEME_RK3IF, true><<<(unsigned)nblk, 256, 0, s>>>(
+                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, c->stat_part);
+            LAUNCH_CK(c);
+            c->launches++;
+            k_stats_final<<<1, STAT_SUMS * 32, 0, s>>>(c->stat_part, (int)nblk, stats_dst);
+            LAUNCH_CK(c);
+            return GNSS_OK;
+        }
         if (uc.scheme == GNSS_SCHEME_CNAB2)
             k_update<T, GNSS_SCHEME_CNAB2><<<(unsigned)nblk, 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz,
                                                                         c->ncp, uc, full_rows);
@@ -634,11 +653,12 @@ static UpdCoef base_coef(const gnss_ctx *c) {
 }
 
 template <typename T>
-static gnss_status step_t(gnss_ctx *c, const gnss_fields *state, const gnss_fields *hist, int euler, cudaStream_t s) {
+static gnss_status step_t(gnss_ctx *c, const gnss_fields *state, const gnss_fields *hist, int euler, cudaStream_t s,
+                          double *stats_dst = nullptr) {
     UpdCoef uc = base_coef(c);
     if (c->cfg.scheme == GNSS_SCHEME_CNAB2) {
         uc.euler = euler ? 1 : 0;
-        return nonlinear_and_update<T>(c, state, nullptr, hist, uc, s);
+        return nonlinear_and_update<T>(c, state, nullptr, hist, uc, s, stats_dst);
     }
     // IF-RK3: the history lives in context scratch after the step's quantities
     gnss_status st = ensure_scratch_step(c);
@@ -652,13 +672,15 @@ static gnss_status step_t(gnss_ctx *c, const gnss_fields *state, const gnss_fiel
         uc.gam = gam[k];
         uc.zet_next = zet[k + 1];
         uc.alph = gam[k] + zet[k];
-        st = nonlinear_and_update<T>(c, state, hb, nullptr, uc, s);
+        st = nonlinear_and_update<T>(c, state, hb, nullptr, uc, s, k == 2 ? stats_dst : nullptr);
         if (st) return st;
     }
     return GNSS_OK;
 }
 
 // ============================================================== statistics
+static void stats_of_sums(const gnss_ctx *c, const double *h, double *out);
+
 template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields *st, double *out, cudaStream_t s) {
     FieldSet<T> F{};
     void *sp[5] = {st->u, st->v, st->w, st->s, st->c};
@@ -673,10 +695,16 @@ template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields 
     CK(c, cudaStreamSynchronize(s));
     gnss_status chk = gnss_check(c, s);
     if (chk) return chk;
+    stats_of_sums(c, c->stat_host, out);
+    return GNSS_OK;
+}
+
+// The GNSS_NSTATS statistics from the STAT_SUMS spectral sums (the
+// normalisations of calcTurbStats, statistics.cu:1494-1845).
+static void stats_of_sums(const gnss_ctx *c, const double *h, double *out) {
     const gnss_config &k = c->cfg;
     const double nn = (double)k.nx * k.ny * k.nz;
     const double n2 = nn * nn;
-    const double *h = c->stat_host;
     out[GNSS_STAT_KE] = (h[0] / n2) / 2.0;
     out[GNSS_STAT_VRMS2] = (h[0] / n2) / 3.0;
     out[GNSS_STAT_EPS] = k.nu_stats * (h[1] / n2);
@@ -684,7 +712,6 @@ template <typename T> static gnss_status stats_t(gnss_ctx *c, const gnss_fields 
     out[GNSS_STAT_CHI_C] = 2.0 * (k.nu_stats / k.sc_c) * (h[3] / n2);
     out[GNSS_STAT_VAR_S] = h[4] / n2;
     out[GNSS_STAT_VAR_C] = h[5] / n2;
-    return GNSS_OK;
 }
 
 // calcTurbStats_mgpu (statistics.cu:2039-2156): spectral sums; the vorticity
@@ -1090,6 +1117,10 @@ gnss_status gnss_destroy(gnss_ctx *c) {
     if (c->turb_host) cudaFreeHost(c->turb_host);
     if (c->d_err) cudaFree(c->d_err);
     if (c->res) cudaFree(c->res);
+    if (c->run_sums) cudaFree(c->run_sums);
+    if (c->run_sums_host) cudaFreeHost(c->run_sums_host);
+    for (cudaEvent_t e : c->side_ev) if (e) cudaEventDestroy(e);
+    if (c->side) cudaStreamDestroy(c->side);
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     delete c;
     return GNSS_OK;
@@ -1331,6 +1362,111 @@ gnss_status gnss_stats(gnss_ctx *c, const gnss_fields *state, double *out, void 
     return PREC_CALL(c, stats_t, c, state, out, S(stream));
 }
 
+// Strided copy of the sub-box ky in [y0, y0 + ny) x kx in [x0, x0 + nx) x
+// kz in [z0, z0 + nz) of one spectral field ([ky][kx][nz2]); nothing when a
+// count is zero.  Adds the bytes copied to *bytes.
+static cudaError_t copy_sub_box(const gnss_ctx *c, void *dst, const void *src, int y0, int ny, int x0, int nx, int z0,
+                                int nz, cudaMemcpyKind kind, cudaStream_t s, size_t *bytes) {
+    if (ny <= 0 || nx <= 0 || nz <= 0) return cudaSuccess;
+    const size_t pitch = (size_t)c->g.nz2 * c->elem;
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<void *>(src), pitch, pitch, (size_t)c->g.nx);
+    p.dstPtr = make_cudaPitchedPtr(dst, pitch, pitch, (size_t)c->g.nx);
+    p.srcPos = make_cudaPos((size_t)z0 * c->elem, (size_t)x0, (size_t)y0);
+    p.dstPos = p.srcPos;
+    p.extent = make_cudaExtent((size_t)nz * c->elem, (size_t)nx, (size_t)ny);
+    p.kind = kind;
+    *bytes += p.extent.width * p.extent.height * p.extent.depth;
+    return cudaMemcpy3DAsync(&p, s);
+}
+
+// Index ranges [first, first + count) of the kept indices of one axis, and
+// the one range of dropped indices (count 0 when every index is kept).
+static int keep_ranges(const KeepMap &m, int first[2], int count[2], int *drop_first, int *drop_count) {
+    if (m.K < 0) {
+        first[0] = 0;
+        count[0] = m.n;
+        *drop_first = *drop_count = 0;
+        return 1;
+    }
+    first[0] = 0;
+    count[0] = m.K + 1;
+    first[1] = m.n - m.K;   // K < n / 2: disjoint from the first range
+    count[1] = m.K;
+    *drop_first = m.K + 1;
+    *drop_count = m.n - 2 * m.K - 1;
+    return m.K > 0 ? 2 : 1;
+}
+
+// Copies of one spectral field restricted to the kept box (kept ky x kept kx
+// x kz < nkz, up to four strided copies; inside = true) or to its complement
+// (up to seven; inside = false).  The box holds every mode that the dealias
+// mask (solver.cu:36) keeps, and a step never writes outside it, so after a
+// dealias the complement is zero for the rest of a run.
+static cudaError_t copy_box(const gnss_ctx *c, void *dst, const void *src, bool inside, cudaMemcpyKind kind,
+                            cudaStream_t s, size_t *bytes) {
+    const Geom &g = c->g;
+    int yf[2], yn[2], xf[2], xn[2], yd0, ydn, xd0, xdn;
+    const int ny_r = keep_ranges(c->ky_keep, yf, yn, &yd0, &ydn);
+    const int nx_r = keep_ranges(c->kx_keep, xf, xn, &xd0, &xdn);
+    cudaError_t e = cudaSuccess;
+    auto put = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    if (!inside) put(copy_sub_box(c, dst, src, yd0, ydn, 0, g.nx, 0, g.nz2, kind, s, bytes));
+    for (int a = 0; a < ny_r; ++a) {
+        if (!inside) put(copy_sub_box(c, dst, src, yf[a], yn[a], xd0, xdn, 0, g.nz2, kind, s, bytes));
+        for (int b = 0; b < nx_r; ++b) {
+            if (inside) put(copy_sub_box(c, dst, src, yf[a], yn[a], xf[b], xn[b], 0, c->nkz, kind, s, bytes));
+            else put(copy_sub_box(c, dst, src, yf[a], yn[a], xf[b], xn[b], c->nkz, g.nz2 - c->nkz, kind, s, bytes));
+        }
+    }
+    return e;
+}
+
+gnss_status gnss_run_host_bytes(gnss_ctx *c, size_t *h2d, size_t *d2h) {
+    if (!c || !h2d || !d2h) return GNSS_ERR_INVALID;
+    const int nf = 3 + c->cfg.n_scalars;
+    int yf[2], yn[2], xf[2], xn[2], d0, dn;
+    const int ny_r = keep_ranges(c->ky_keep, yf, yn, &d0, &dn), nx_r = keep_ranges(c->kx_keep, xf, xn, &d0, &dn);
+    size_t rows = 0;
+    for (int a = 0; a < ny_r; ++a)
+        for (int b = 0; b < nx_r; ++b) rows += (size_t)yn[a] * xn[b];
+    *h2d = (size_t)nf * rows * (size_t)c->nkz * c->elem;
+    *d2h = (size_t)nf * c->nspec * c->elem;
+    return GNSS_OK;
+}
+
+// gnss_run_host after the upload: the download of the modes outside the
+// kept box on the side stream (zero from the dealias to the end of the run,
+// so it overlaps the steps; it writes parts of host_out that the upload does
+// not read, and host_out may alias host_in), the steps with their statistics
+// summed by the update, then the statistics and the kept box downloaded.
+static gnss_status run_host_steps(gnss_ctx *c, const gnss_fields *st, const gnss_fields *hi, char *out, int n_steps,
+                                  int first_euler, double *stats_out, cudaStream_t s) {
+    const int nf = 3 + c->cfg.n_scalars;
+    const size_t fb = c->nspec * c->elem;
+    void *const sp[5] = {st->u, st->v, st->w, st->s, st->c};
+    size_t moved = 0;
+    CK(c, cudaEventRecord(c->side_ev[0], s));
+    CK(c, cudaStreamWaitEvent(c->side, c->side_ev[0], 0));
+    for (int q = 0; q < nf; ++q)
+        CK(c, copy_box(c, out + (size_t)q * fb, sp[q], false, cudaMemcpyDeviceToHost, c->side, &moved));
+    CK(c, cudaEventRecord(c->side_ev[1], c->side));
+    for (int i = 0; i < n_steps; ++i) {
+        const int euler = (i == 0 && first_euler) ? 1 : 0;
+        double *dst = stats_out ? c->run_sums + (size_t)i * STAT_SUMS : nullptr;
+        gnss_status r = PREC_CALL(c, step_t, c, st, hi, euler, s, dst);
+        if (r) return r;
+    }
+    if (stats_out && n_steps > 0)
+        CK(c, cudaMemcpyAsync(c->run_sums_host, c->run_sums, sizeof(double) * STAT_SUMS * (size_t)n_steps,
+                              cudaMemcpyDeviceToHost, s));
+    for (int q = 0; q < nf; ++q)
+        CK(c, copy_box(c, out + (size_t)q * fb, sp[q], true, cudaMemcpyDeviceToHost, s, &moved));
+    CK(c, cudaStreamWaitEvent(s, c->side_ev[1], 0));
+    CK(c, cudaStreamSynchronize(s));
+    return GNSS_OK;
+}
+
 gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int n_steps, int first_euler,
                           double *stats_out, void *stream) {
     if (!c || !host_in || !host_out || n_steps < 0) return fail(c, GNSS_ERR_INVALID, "bad argument");
@@ -1345,8 +1481,31 @@ gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int 
         }
         c->owned_bytes += 2 * (size_t)nf * fb;
     }
+    if (stats_out && n_steps > c->run_sums_cap) {   // per-step sums, read back once after the last step
+        if (c->run_sums) cudaFree(c->run_sums);
+        if (c->run_sums_host) cudaFreeHost(c->run_sums_host);
+        c->run_sums = nullptr;
+        c->run_sums_host = nullptr;
+        c->run_sums_cap = 0;
+        const size_t b = sizeof(double) * STAT_SUMS * (size_t)n_steps;
+        if (cudaMalloc(&c->run_sums, b) != cudaSuccess || cudaMallocHost(&c->run_sums_host, b) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GNSS_ERR_NOMEM, "cannot allocate statistics buffers");
+        }
+        c->run_sums_cap = n_steps;
+    }
+    if (!c->side) {
+        if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->side_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->side_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GNSS_ERR_CUDA, "cannot create the copy stream");
+        }
+    }
     cudaStream_t s = S(stream);
     char *base = reinterpret_cast<char *>(c->res);
+    char *out = static_cast<char *>(host_out);
+    const char *in = static_cast<const char *>(host_in);
     gnss_fields st{}, hi{};
     void **sp[5] = {&st.u, &st.v, &st.w, &st.s, &st.c};
     void **hp[5] = {&hi.u, &hi.v, &hi.w, &hi.s, &hi.c};
@@ -1354,23 +1513,29 @@ gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int 
         *sp[q] = base + (size_t)q * fb;
         *hp[q] = base + (size_t)(nf + q) * fb;
     }
-    CK(c, cudaMemcpyAsync(base, host_in, (size_t)nf * fb, cudaMemcpyHostToDevice, s));
-    CK(c, cudaMemsetAsync(base + (size_t)nf * fb, 0, (size_t)nf * fb, s));
-    for (int q = 0; q < nf; ++q) {   // as the reference does before its loop (main.cu:156)
+    if (!al_fields(c, &st) || !al_fields(c, &hi)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
+    // The state zeroed, the kept box of each field uploaded and dealiased, as
+    // the reference does before its loop (main.cu:156).  The history starts
+    // at zero; the Euler step of CN/AB2 writes all of its kept box (the only
+    // part ever read) and IF-RK3 keeps its own, so it is cleared only for a
+    // CN/AB2 run that starts with AB2.
+    const bool clear_hist = c->cfg.scheme == GNSS_SCHEME_CNAB2 && !first_euler;
+    CK(c, cudaMemsetAsync(base, 0, (clear_hist ? 2 : 1) * (size_t)nf * fb, s));
+    size_t moved = 0;
+    for (int q = 0; q < nf; ++q) {
+        CK(c, copy_box(c, *sp[q], in + (size_t)q * fb, true, cudaMemcpyHostToDevice, s, &moved));
         gnss_status r = gnss_dealias(c, *sp[q], stream);
         if (r) return r;
     }
-    for (int i = 0; i < n_steps; ++i) {
-        gnss_status r = gnss_step(c, &st, &hi, (i == 0 && first_euler) ? 1 : 0, stream);
-        if (r) return r;
-        if (stats_out) {
-            r = gnss_stats(c, &st, stats_out + (size_t)i * GNSS_NSTATS, stream);
-            if (r) return r;
-        }
-    }
-    CK(c, cudaMemcpyAsync(host_out, base, (size_t)nf * fb, cudaMemcpyDeviceToHost, s));
-    CK(c, cudaStreamSynchronize(s));
-    return gnss_check(c, stream);
+    gnss_status r = run_host_steps(c, &st, &hi, out, n_steps, first_euler, stats_out, s);
+    cudaStreamSynchronize(c->side);   // no copy into host_out outlives the call, also after an error
+    if (r) return r;
+    gnss_status chk = gnss_check(c, stream);
+    if (chk) return chk;
+    if (stats_out)
+        for (int i = 0; i < n_steps; ++i)
+            stats_of_sums(c, c->run_sums_host + (size_t)i * STAT_SUMS, stats_out + (size_t)i * GNSS_NSTATS);
+    return GNSS_OK;
 }
 
 

@@ -545,6 +545,11 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
     }
 }
 
+// statistics reductions (k_update with STATS, k_stats_partial, k_stats_final)
+constexpr int STAT_SUMS = 6;
+constexpr int STAT_BLOCKS = 1184;   // 8 x 148 SMs
+constexpr int STAT_THREADS = 256;
+
 // ------------------------------------------------------------ spectral update
 struct UpdCoef {
     int nf;           // fields updated: 3 + n_scalars
@@ -568,12 +573,20 @@ struct UpdCoef {
 // are written as zero instead (the first step of a run: it clears whatever
 // the history held there); modes outside the box are never touched.  Every
 // load of a mode is issued before its first store.
-template <typename T, int SCHEME>
+//
+// With STATS, the kernel also sums, over the modes it writes, the spectral
+// statistics of the new state (the six sums of k_stats_partial: the full
+// spectrum through the kz mirror, statistics.cu:1494-1845) and writes one row
+// of STAT_SUMS partials per block to `partial`; for a state that is zero
+// outside the dealiasing sphere (the precondition of the step) they equal the
+// sums over the whole field.
+template <typename T, int SCHEME, bool STATS = false>
 __global__ void __launch_bounds__(256)
 k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
          const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
-         UpdCoef c, int full_rows) {
+         UpdCoef c, int full_rows, double *__restrict__ partial = nullptr) {
     using V = V2<T>;
+    double acc[STATS ? STAT_SUMS : 1] = {};
     const int nkx = kx_keep.count(), nky = ky_keep.count();
     const int nrows = nky * nkx;
     const int lane = threadIdx.x & 31;
@@ -642,8 +655,10 @@ k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ Fiel
                     R[q][1] = -(double)a[q].y;
                 }
             }
+            V sv[STATS ? 5 : 1];   // the stored new state (the statistics read these values)
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
+                if constexpr (STATS) sv[q] = V{T(0), T(0)};
                 if (q >= nf) break;
                 const double fr = (double)f[q].x, fi = (double)f[q].y;
                 if constexpr (SCHEME == 0) {
@@ -660,15 +675,48 @@ k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ Fiel
                         ni = (am * fi + c.dt * (1.5 * R[q][1] - 0.5 * (double)h[q].y)) * ib;
                     }
                     state.p[q][idx] = V{(T)nr, (T)ni};
+                    if constexpr (STATS) sv[q] = V{(T)nr, (T)ni};
                     hist.p[q][idx] = V{(T)R[q][0], (T)R[q][1]};   // updateKernel_mgpu (solver.cu:618-637)
                 } else {
                     const double E = exp(-c.nu[q] * ksq * c.alph * c.dt);
                     const double nr = E * (fr + c.gam * c.dt * R[q][0] + (double)h[q].x);
                     const double ni = E * (fi + c.gam * c.dt * R[q][1] + (double)h[q].y);
                     state.p[q][idx] = V{(T)nr, (T)ni};
+                    if constexpr (STATS) sv[q] = V{(T)nr, (T)ni};
                     hist.p[q][idx] = V{(T)(c.zet_next * c.dt * E * R[q][0]), (T)(c.zet_next * c.dt * E * R[q][1])};
                 }
             }
+            if constexpr (STATS) {   // sums of the stored (T) values, as k_stats_partial reads them
+                const double wt = (kzi == 0 || 2 * kzi == g.nz) ? 1.0 : 2.0;
+                const bool origin = kxi == 0 && kyi == 0 && kzi == 0;
+                double m[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) m[q] = (double)sv[q].x * sv[q].x + (double)sv[q].y * sv[q].y;
+                const double e = m[0] + m[1] + m[2];
+                acc[0] += wt * e;
+                acc[1] += wt * ksq * e;
+                acc[2] += wt * ksq * m[3];
+                acc[3] += wt * ksq * m[4];
+                if (!origin) {
+                    acc[4] += wt * m[3];
+                    acc[5] += wt * m[4];
+                }
+            }
+        }
+    }
+    if constexpr (STATS) {   // fixed-order block reduction: warp shuffles, then the block's warps in order
+        __shared__ double red[STAT_SUMS][8];
+#pragma unroll
+        for (int q = 0; q < STAT_SUMS; ++q) {
+            double v = acc[q];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) red[q][threadIdx.x >> 5] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < STAT_SUMS) {
+            double v = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+            partial[blockIdx.x * STAT_SUMS + threadIdx.x] = v;
         }
     }
 }
@@ -677,9 +725,6 @@ k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ Fiel
 // Six sums per thread, Kahan-compensated, reduced in a fixed tree order per
 // block; the partials are summed in a fixed order by one block.  The result
 // is independent of scheduling (unlike atomicAdd in statistics.cu:1555).
-constexpr int STAT_SUMS = 6;
-constexpr int STAT_BLOCKS = 1184;   // 8 x 148 SMs
-constexpr int STAT_THREADS = 256;
 
 struct Kahan {
     double s = 0.0, c = 0.0;

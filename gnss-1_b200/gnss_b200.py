@@ -99,6 +99,7 @@ _SIGS = {
     "gnss_step": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields), ctypes.c_int, _VP],
     "gnss_stats": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_run_host": [_VP, _VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), _VP],
+    "gnss_run_host_bytes": [_VP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)],
     "gnss_launch_count": [_VP],
     "gnss_check": [_VP, _VP],
     "gnss_forward_noalloc": [ctypes.POINTER(GnssConfig), _VP, _VP],
@@ -378,6 +379,12 @@ class Context:
                 else ctypes.cast(stats.data_ptr(), ctypes.POINTER(ctypes.c_double))
         self._ck(self.lib.gnss_run_host(self._h, _host_ptr(host_in), _host_ptr(host_out), int(n_steps),
                                         int(bool(first_euler)), sp, _stream(stream)), "gnss_run_host")
+
+    def run_host_bytes(self) -> tuple:
+        """(host-to-device, device-to-host) state bytes one run_host call copies."""
+        h2d, d2h = ctypes.c_size_t(), ctypes.c_size_t()
+        self._ck(self.lib.gnss_run_host_bytes(self._h, ctypes.byref(h2d), ctypes.byref(d2h)), "gnss_run_host_bytes")
+        return h2d.value, d2h.value
 
     def check(self, stream=None) -> None:
         """Synchronise and raise if a bounded device wait timed out."""

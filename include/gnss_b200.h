@@ -184,9 +184,20 @@ gnss_status gnss_turb_stats(gnss_ctx *ctx, const gnss_fields *state, gnss_turb *
  * GNSS_SCHEME_CNAB2; hist starts at zero), records the statistics after each
  * step into stats_out (n_steps * GNSS_NSTATS doubles, may be NULL) and copies
  * the final state back into host_state_out (may alias host_state_in).
- * Synchronises the stream before returning. */
+ * Only the modes a dealias can keep (the box |kx|, |ky|, |kz| <= the
+ * truncation radius) are read from host_state_in; the result is the same as
+ * uploading everything.  The modes outside that box, zero after the dealias,
+ * are written to host_state_out on a second stream while the steps run, the
+ * box after the last step.  The statistics are summed by the update kernel of
+ * each step and read back once, after the last step; they equal gnss_stats
+ * of the same state to round-off.  Synchronises the stream before returning. */
 gnss_status gnss_run_host(gnss_ctx *ctx, const void *host_state_in, void *host_state_out, int n_steps,
                           int first_euler, double *stats_out, void *stream);
+
+/* State bytes one gnss_run_host call copies host-to-device (the kept box of
+ * every field) and device-to-host (the whole packed state), statistics
+ * excluded.  No counterpart in the reference. */
+gnss_status gnss_run_host_bytes(gnss_ctx *ctx, size_t *h2d_bytes, size_t *d2h_bytes);
 
 /* Synchronises the stream and reports GNSS_ERR_TIMEOUT if any kernel of this
  * context gave up a bounded wait since the last check (the flag is then

@@ -3,8 +3,11 @@
 Both are schedulers over the same per-jet step (solver_ps, solver.cu:700-765):
 a member of an ensemble, or a request in a server, must end bit-identical to
 the same jet run alone through gnss_run_host (upload, dealias as main.cu:156,
-Euler first step, AB2 after), whatever else runs beside it.
+Euler first step, AB2 after), whatever else runs beside it.  Statistics agree
+to round-off: gnss_run_host sums them inside the update kernel.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -58,7 +61,7 @@ def test_ensemble_members_match_alone(torch_cuda):
     for i, (c, a) in enumerate(zip(cfgs, init)):
         ref, rstats = _alone(G, c, a, 11)
         assert np.array_equal(got[i][0], ref), f"member {i} differs from the jet run alone"
-        assert got[i][1]["ke"] == rstats[0]
+        assert math.isclose(got[i][1]["ke"], rstats[0], rel_tol=1e-12)   # same state, other summation order
 
 
 @pytest.mark.gpu
@@ -111,7 +114,8 @@ def test_server_result_same_alone_and_in_the_mix(torch_cuda):
         rep = srv.report()
     assert np.array_equal(alone, ref)
     assert np.array_equal(mixed, ref)
-    assert s_alone["ke"] == rstats[0] and s_mixed["ke"] == rstats[0]
+    assert s_alone["ke"] == s_mixed["ke"]
+    assert math.isclose(s_alone["ke"], rstats[0], rel_tol=1e-12)
     assert times[0] <= times[1] <= times[2]
     assert rep["completed"] == 1 + len(others) and rep["failed"] == 0
     assert rep["active_max"] >= 2     # requests overlapped on the device
