@@ -12,9 +12,10 @@
 //           DFT across the lanes of a group with shuffles.
 // A line therefore crosses shared memory once per transform (instead of once
 // per radix-8 stage), the C2R packing is done while loading the registers,
-// and the twiddles of step A are products of four table powers.  Physical
-// values are exchanged between warps through one bank of lines; the whole
-// block forms the products into the scratch lines of the forward warps.
+// and the twiddles of step A are products of four table powers.  Each warp
+// leaves its physical quantity in its own scratch line, where the other warps
+// read it; the whole block forms the products in place, into the lines of the
+// forward warps.
 #pragma once
 #include "kernels.cuh"
 
@@ -97,9 +98,10 @@ template <typename T, int N> struct ZRCfg {
     __host__ __device__ static constexpr int pidx(int n) { return n + PADP * (n >> 6); }
     static_assert(E == 8 || E == 16, "register z transform serves N = 256 and 512");
     static_assert(SCR >= PL, "scratch holds a padded line");
-    // twiddle powers, physical lines, scratch lines, raw staging, mbarrier (16 B), kz table (ncp T)
+    // twiddle powers, scratch lines (one per warp; they also hold the physical
+    // lines and the products), raw staging, mbarrier (16 B), kz table (ncp T)
     __host__ __device__ static constexpr int smem_bytes(int nph, int nraw, int ncp) {
-        return (LOGE * 32 + nph * PL + nph * SCR + nraw * 2 * ncp) * (int)sizeof(V2<T>) + 16 + ncp * (int)sizeof(T);
+        return (LOGE * 32 + nph * SCR + nraw * 2 * ncp) * (int)sizeof(V2<T>) + 16 + ncp * (int)sizeof(T);
     }
 };
 
@@ -253,35 +255,38 @@ __device__ __forceinline__ void zr_pack(int lane, V2<T> *x, const ZRecipe rc, co
     }
 }
 
-// Pointwise products of one line pair by the whole block: point n of product
-// f goes to element pidx(n) of line f of `out` (the scratch lines of the
-// forward warps, stride SCR).  Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3,
+// Pointwise products of one line pair by the whole block, in place: the
+// physical quantities are element pidx(n) of the scratch lines (stride SCR),
+// and product f replaces quantity f there (the lines of the forward warps).
+// Each point is read in full by one thread before that thread writes it;
+// quantities 0 .. 4 are read before any product is written, and the products
+// go to lines 0 .. 4 only.  Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3,
 // 6 sx, 7 sy, 8 sz, [9 cx, 10 cy, 11 cz], [12 c, 13 lap s]; products as
 // zphys_products: (w x u) (crossProductKernel_mgpu, solver.cu:139-164),
 // u . grad s (dotKernel_mgpu, solver.cu:342-356) and the colloid term
 // (colloidAdvectionKernel_mgpu, solver.cu:374-388).
 template <typename T, int N, int NPH>
-__device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alpha) {
+__device__ __forceinline__ void zr_products(V2<T> *lines, T alpha) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
-    constexpr int PL = Z::PL, SCR = Z::SCR;
+    constexpr int SCR = Z::SCR;
     constexpr bool has_c = NPH >= 12, has_al = NPH >= 14;
     for (int n = threadIdx.x; n < N; n += blockDim.x) {
         const int pn = Z::pidx(n);
-        const V *p = phys + pn;
-        const V u = p[0 * PL], v = p[1 * PL], w = p[2 * PL];
-        const V o1 = p[3 * PL], o2 = p[4 * PL], o3 = p[5 * PL];
-        const V sx = p[6 * PL], sy = p[7 * PL], sz = p[8 * PL];
-        V *o = out + pn;
+        const V *p = lines + pn;
+        const V u = p[0 * SCR], v = p[1 * SCR], w = p[2 * SCR];
+        const V o1 = p[3 * SCR], o2 = p[4 * SCR], o3 = p[5 * SCR];
+        const V sx = p[6 * SCR], sy = p[7 * SCR], sz = p[8 * SCR];
+        V *o = lines + pn;
         o[0 * SCR] = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
         o[1 * SCR] = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
         o[2 * SCR] = V{o1.x * v.x - o2.x * u.x, o1.y * v.y - o2.y * u.y};
         o[3 * SCR] = V{u.x * sx.x + v.x * sy.x + w.x * sz.x, u.y * sx.y + v.y * sy.y + w.y * sz.y};
         if constexpr (has_c) {
-            const V cx = p[9 * PL], cy = p[10 * PL], cz = p[11 * PL];
+            const V cx = p[9 * SCR], cy = p[10 * SCR], cz = p[11 * SCR];
             const V adv = V{u.x * cx.x + v.x * cy.x + w.x * cz.x, u.y * cx.y + v.y * cy.y + w.y * cz.y};
             if constexpr (has_al) {
-                const V cc = p[12 * PL], ls = p[13 * PL];
+                const V cc = p[12 * SCR], ls = p[13 * SCR];
                 const V dr = V{ls.x * cc.x + cx.x * sx.x + cy.x * sy.x + cz.x * sz.x,
                                ls.y * cc.y + cx.y * sx.y + cy.y * sy.y + cz.y * sz.y};
                 o[4 * SCR] = V{alpha * dr.x + adv.x, alpha * dr.y + adv.y};
@@ -297,18 +302,17 @@ __device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alp
 // cp.async.bulk (CTA-local, no multicast) while the current pair is
 // processed; a wait that times out sets bit 0 of *err and the block stops.
 template <typename T, int N, int NPH, int NRAW>
-__global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? 2 : 1)
+__global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? 3 : 1)
 k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
        int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
-    constexpr int E = Z::E, PL = Z::PL, SCR = Z::SCR;
+    constexpr int E = Z::E, SCR = Z::SCR;
     const int rawf = 2 * ncp;
     const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
-    V *phys = tws + Z::LOGE * 32;
-    V *scr_all = phys + NPH * PL;
+    V *scr_all = tws + Z::LOGE * 32;
     V *raw = scr_all + NPH * SCR;
     uint64_t *bar = reinterpret_cast<uint64_t *>(raw + NRAW * rawf);
     T *tkz = reinterpret_cast<T *>(bar + 2);   // kz wavenumbers of the kept modes (ncp entries)
@@ -335,8 +339,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
     if (threadIdx.x == 0) issue(pair);
     unsigned parity = 0;
     const ZRecipe rc = zr.q[warp];
-    V *scr = scr_all + warp * SCR;
-    V *myphys = phys + warp * PL;
+    V *scr = scr_all + warp * SCR;   // transposes, then this warp's physical quantity
     for (; pair < npairs; pair += gridDim.x) {
         const bool ok = mbar_wait_bounded(bar, parity);
         if (__syncthreads_or(!ok)) {
@@ -353,11 +356,11 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
             fence_proxy_async_smem();
             issue(pair + gridDim.x);
         }
-        zr_fft<T, N, +1>(lane, x, scr, tws);
+        zr_fft<T, N, +1>(lane, x, scr, tws);   // ends its scratch reads with __syncwarp
 #pragma unroll
-        for (int q = 0; q < E; ++q) myphys[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
+        for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
         __syncthreads();   // every physical quantity on chip
-        zr_products<T, N, NPH>(phys, scr_all, alpha);
+        zr_products<T, N, NPH>(scr_all, alpha);
         __syncthreads();   // products in the scratch lines of warps 0 .. nout-1
         if (warp < nout) {   // z R2C of product `warp`, written over raw field `warp` of the pair
 #pragma unroll
