@@ -130,7 +130,8 @@ def measured_peaks() -> dict:
 
 
 # ------------------------------------------------------------------ our arm
-VARIANTS = {"auto": 0, "register": 1, "staged": 2}
+VARIANTS = {"auto": 0, "register": 1, "staged": 2, "warpspec": 3}
+ZNAMES = tuple(VARIANTS)   # variant names by value
 
 
 def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None, variants=None):
@@ -273,8 +274,8 @@ def run_ensemble(G, torch, dev, steps, branches=8) -> dict:
                         "FP32, dt 1e-3, cnab2",
             "graph": f"{chunk} steps of all 32 members per CUDA graph launch, {branches} branches",
             "gpu_launches_per_step": lps, "autotune_s": round(t_tune, 2),
-            "autotune_choices": {str(n): {"z": ("auto", "register", "staged")[choices[ENSEMBLE_SIZES.index(n)] & 3],
-                                          "pass": ("auto", "register", "staged")[choices[ENSEMBLE_SIZES.index(n)] >> 2]}
+            "autotune_choices": {str(n): {"z": ZNAMES[choices[ENSEMBLE_SIZES.index(n)] & 3],
+                                          "pass": ZNAMES[choices[ENSEMBLE_SIZES.index(n)] >> 2]}
                                  for n in sorted(set(ENSEMBLE_SIZES))},
             "clocks": clk.summary()}
 
@@ -506,7 +507,7 @@ def main():
     ap.add_argument("--no-fp64-leg", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--z-variant", choices=tuple(VARIANTS), default="auto")
-    ap.add_argument("--pass-variant", choices=tuple(VARIANTS), default="auto")
+    ap.add_argument("--pass-variant", choices=("auto", "register", "staged"), default="auto")
     ap.add_argument("--no-error-check", action="store_true")
     ap.add_argument("--error-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")

@@ -60,6 +60,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
     return false;
 }
 
+// Named barrier `id` (1..15; 0 is __syncthreads) over `nthreads` threads,
+// whole warps; true on every participant when pred is true on any of them.
+__device__ __forceinline__ bool bar_named_or(unsigned id, unsigned nthreads, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
 // ---------------------------------------------------------------- cp.async
 // Per-thread asynchronous copies global -> shared (LDGSTS).  src_bytes = 0
 // fills the destination with zeros without reading the source.

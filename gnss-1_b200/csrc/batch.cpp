@@ -276,23 +276,28 @@ gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream) {
 gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     if (!e || steps < 1) return GNSS_ERR_INVALID;
     if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
-    using Key = std::tuple<int, int, int, int, int, int>;
+    using Key = std::tuple<int, int, int, int, int, int, bool>;
     std::map<Key, int> best;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     gnss_status st = GNSS_OK;
-    const int variants[2] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED};
+    const int zvariants[3] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED, GNSS_VARIANT_WARPSPEC};
+    const int pvariants[2] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED};
+    auto key_of = [](const gnss_config &c) {
+        return Key{c.nx, c.ny, c.nz, c.precision, c.n_scalars, c.scheme, c.alpha != 0.0};
+    };
     for (Member &mb : e->m) {
-        const Key k{mb.cfg.nx, mb.cfg.ny, mb.cfg.nz, mb.cfg.precision, mb.cfg.n_scalars, mb.cfg.scheme};
+        const Key k = key_of(mb.cfg);
         if (best.count(k)) continue;
         const cudaStream_t bs = e->streams[mb.branch];
         float tbest = 0.f;
         int vbest = 0;
-        for (int combo = 0; combo < 4; ++combo) {
-            const int v = variants[combo & 1] + 4 * variants[combo >> 1];   // z variant + 4 * pass variant
-            if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, variants[combo & 1])) ||
-                (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, variants[combo >> 1])))
+        for (int combo = 0; combo < 6; ++combo) {
+            const int zv = zvariants[combo % 3], pv = pvariants[combo / 3];
+            const int v = zv + 4 * pv;   // z variant + 4 * pass variant
+            if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, zv)) ||
+                (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, pv)))
                 break;
             if ((st = gnss_step(mb.ctx, &mb.state, &mb.hist, 1, bs))) break;   // warm-up
             cudaEventRecord(t0, bs);
@@ -315,7 +320,7 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     if (st) return st;
     for (size_t i = 0; i < e->m.size(); ++i) {
         Member &mb = e->m[i];
-        const int v = best[Key{mb.cfg.nx, mb.cfg.ny, mb.cfg.nz, mb.cfg.precision, mb.cfg.n_scalars, mb.cfg.scheme}];
+        const int v = best[key_of(mb.cfg)];
         if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v & 3)) ||
             (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, v >> 2)))
             return st;

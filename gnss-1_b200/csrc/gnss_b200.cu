@@ -270,6 +270,35 @@ template <typename T, int N> struct Launch {
             return cudaErrorNotSupported;
         }
     }
+    // warp-specialised register z kernel (FP32, 9 quantities, 4 products)
+    static cudaError_t zws_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
+                             T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s) {
+        if constexpr ((N == 256 || N == 512) && sizeof(T) == 4) {
+            const int smem = ZRCfg<T, N>::smem_bytes_ws(ZWS_NPH, ZWS_NOUT, 10, ncp);
+            auto kern = k_zws<T, N, ZWS_NPH, 10>;
+            cudaError_t e = prep_smem(kern, smem);
+            if (e != cudaSuccess) return e;
+            const int nt = (ZWS_NPH + ZWS_NOUT) * 32;
+            const int per_sm = blocks_per_sm(kern, nt, smem);
+            const long long npairs = nlines / 2;
+            long long grid = (long long)per_sm * nsm;
+            if (grid > npairs) grid = npairs;
+            kern<<<(unsigned)grid, nt, smem, s>>>(f, zr, nout, npairs, ncp, nkz, scale, alpha, dkz,
+                                                   reinterpret_cast<const V2<T> *>(tw), err);
+            return cudaGetLastError();
+        } else {
+            (void)f; (void)zr; (void)nout; (void)nlines; (void)ncp; (void)nkz; (void)scale; (void)alpha; (void)dkz;
+            (void)tw; (void)err; (void)nsm; (void)s;
+            return cudaErrorNotSupported;
+        }
+    }
+    static bool zws_fits(int nph, int nraw, int nout, int ncp) {
+        if constexpr ((N == 256 || N == 512) && sizeof(T) == 4)
+            return nph == ZWS_NPH && nraw == 10 && nout == ZWS_NOUT &&
+                   ZRCfg<T, N>::smem_bytes_ws(ZWS_NPH, ZWS_NOUT, 10, ncp) <= ZPCfg<T, N>::SMEM_MAX;
+        else
+            return false;
+    }
     static bool zreg_fits(int nph, int nraw, int ncp) {
         if constexpr (N == 256 || N == 512)
             return ZRCfg<T, N>::smem_bytes(nph, nraw, ncp) <= ZPCfg<T, N>::SMEM_MAX;
@@ -279,6 +308,8 @@ template <typename T, int N> struct Launch {
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
                              unsigned *err, int nsm, cudaStream_t s, int zvariant) {
+        if (zvariant == GNSS_VARIANT_WARPSPEC && zws_fits(nph, nraw, nout, ncp))
+            return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
         if (zvariant != GNSS_VARIANT_STAGED && zreg_fits(nph, nraw, ncp)) {
             if (nph == 9 && nraw == 10)
                 return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
@@ -839,7 +870,8 @@ gnss_status gnss_stage_bytes(const gnss_ctx *c, double *bytes) {
 gnss_status gnss_set_option(gnss_ctx *c, int key, int value) {
     if (!c) return GNSS_ERR_INVALID;
     if (key != GNSS_OPT_ZVARIANT && key != GNSS_OPT_PVARIANT) return fail(c, GNSS_ERR_INVALID, "unknown option %d", key);
-    if (value < GNSS_VARIANT_AUTO || value > GNSS_VARIANT_STAGED)
+    const int top = key == GNSS_OPT_ZVARIANT ? GNSS_VARIANT_WARPSPEC : GNSS_VARIANT_STAGED;
+    if (value < GNSS_VARIANT_AUTO || value > top)
         return fail(c, GNSS_ERR_INVALID, "bad variant %d for option %d", value, key);
     (key == GNSS_OPT_ZVARIANT ? c->zvariant : c->pvariant) = value;
     return GNSS_OK;

@@ -103,6 +103,10 @@ template <typename T, int N> struct ZRCfg {
     __host__ __device__ static constexpr int smem_bytes(int nph, int nraw, int ncp) {
         return (LOGE * 32 + nph * SCR + nraw * 2 * ncp) * (int)sizeof(V2<T>) + 16 + ncp * (int)sizeof(T);
     }
+    // k_zws: one more scratch line per forward warp
+    __host__ __device__ static constexpr int smem_bytes_ws(int nph, int nout, int nraw, int ncp) {
+        return smem_bytes(nph + nout, nraw, ncp);
+    }
 };
 
 // Output slot of a lane group member after the G-point cross-lane DFT.
@@ -255,29 +259,30 @@ __device__ __forceinline__ void zr_pack(int lane, V2<T> *x, const ZRecipe rc, co
     }
 }
 
-// Pointwise products of one line pair by the whole block, in place: the
-// physical quantities are element pidx(n) of the scratch lines (stride SCR),
-// and product f replaces quantity f there (the lines of the forward warps).
-// Each point is read in full by one thread before that thread writes it;
-// quantities 0 .. 4 are read before any product is written, and the products
-// go to lines 0 .. 4 only.  Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3,
+// Pointwise products of one line pair by the whole block: the physical
+// quantities are element pidx(n) of the lines `phys` (stride SCR), product f
+// goes to element pidx(n) of line f of `out` (stride SCR).  out may equal
+// phys (products in place over quantities 0 .. 4): each point is read in full
+// by one thread before that thread writes it, quantities 0 .. 4 are read
+// before any product is written, and products go to lines 0 .. 4 only.
+// Quantities: 0 u, 1 v, 2 w, 3 w1, 4 w2, 5 w3,
 // 6 sx, 7 sy, 8 sz, [9 cx, 10 cy, 11 cz], [12 c, 13 lap s]; products as
 // zphys_products: (w x u) (crossProductKernel_mgpu, solver.cu:139-164),
 // u . grad s (dotKernel_mgpu, solver.cu:342-356) and the colloid term
 // (colloidAdvectionKernel_mgpu, solver.cu:374-388).
 template <typename T, int N, int NPH>
-__device__ __forceinline__ void zr_products(V2<T> *lines, T alpha) {
+__device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alpha) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
     constexpr int SCR = Z::SCR;
     constexpr bool has_c = NPH >= 12, has_al = NPH >= 14;
     for (int n = threadIdx.x; n < N; n += blockDim.x) {
         const int pn = Z::pidx(n);
-        const V *p = lines + pn;
+        const V *p = phys + pn;
         const V u = p[0 * SCR], v = p[1 * SCR], w = p[2 * SCR];
         const V o1 = p[3 * SCR], o2 = p[4 * SCR], o3 = p[5 * SCR];
         const V sx = p[6 * SCR], sy = p[7 * SCR], sz = p[8 * SCR];
-        V *o = lines + pn;
+        V *o = out + pn;
         o[0 * SCR] = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
         o[1 * SCR] = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
         o[2 * SCR] = V{o1.x * v.x - o2.x * u.x, o1.y * v.y - o2.y * u.y};
@@ -295,6 +300,31 @@ __device__ __forceinline__ void zr_products(V2<T> *lines, T alpha) {
             }
         }
     }
+}
+
+// R2C output of one product line: the length-N transform in x (element
+// zr_out_index(lane, q) in x[q]) goes through the warp's scratch line, and the
+// kept modes of the two real lines of the pair are stored as the raw layout
+// ([A: ncp][B: ncp]) at d.
+template <typename T, int N>
+__device__ __forceinline__ void zr_store_r2c(int lane, const V2<T> *x, V2<T> *scr, V2<T> *d, int ncp) {
+    using V = V2<T>;
+    using Z = ZRCfg<T, N>;
+#pragma unroll
+    for (int q = 0; q < Z::E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = x[q];
+    __syncwarp();
+    for (int k = lane; k < ncp; k += 32) {
+        V A = V{T(0), T(0)}, B = V{T(0), T(0)};
+        if (2 * k <= N) {
+            const V zk = scr[Z::pidx(k)];
+            const V zm = scr[Z::pidx((N - k) % N)];
+            A = V{T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
+            B = V{T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
+        }
+        d[k] = A;
+        d[ncp + k] = B;
+    }
+    __syncwarp();   // scratch reused by the next transform
 }
 
 // Persistent: block b handles line pairs b, b + gridDim.x, ...; warp q forms
@@ -360,30 +390,118 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
 #pragma unroll
         for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
         __syncthreads();   // every physical quantity on chip
-        zr_products<T, N, NPH>(scr_all, alpha);
+        zr_products<T, N, NPH>(scr_all, scr_all, alpha);
         __syncthreads();   // products in the scratch lines of warps 0 .. nout-1
         if (warp < nout) {   // z R2C of product `warp`, written over raw field `warp` of the pair
 #pragma unroll
             for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
             __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
-#pragma unroll
-            for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = x[q];
-            __syncwarp();
-            V *d = f.p[warp] + pair * rawf;
-            for (int k = lane; k < ncp; k += 32) {
-                V A = V{T(0), T(0)}, B = V{T(0), T(0)};
-                if (2 * k <= N) {
-                    const V zk = scr[Z::pidx(k)];
-                    const V zm = scr[Z::pidx((N - k) % N)];
-                    A = V{T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
-                    B = V{T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
-                }
-                d[k] = A;
-                d[ncp + k] = B;
-            }
-            __syncwarp();   // scratch reused by the next transform
+            zr_store_r2c<T, N>(lane, x, scr, f.p[warp] + pair * rawf, ncp);
         }
+    }
+}
+
+// Warp-specialised form of k_zreg (same arguments, same results): NPH inverse
+// warps and ZWS_NOUT forward warps per block, each with its own scratch line.
+// Per line pair p, between two block barriers, the inverse warps unpack and
+// transform the quantities of p (each leaving its physical quantity in its
+// own line) while the forward warps transform and store the products of the
+// block's previous pair (held in their own lines); after the first barrier
+// the whole block forms the products of p into the forward warps' lines.
+// Every warp thus runs one length-N transform per pair instead of 4 of 9
+// warps running the forward ones alone.  The raw lines of the next pair are
+// requested as soon as every inverse warp has unpacked (named barrier 1); a
+// wait that times out sets bit 0 of *err and the block stops.  FP32 with 9
+// quantities: 13 warps, 72 registers, two blocks per SM.
+constexpr int ZWS_NPH = 9, ZWS_NOUT = 4;
+template <typename T, int N, int NPH, int NRAW>
+__global__ void __launch_bounds__((ZWS_NPH + ZWS_NOUT) * 32, 2)
+k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
+      int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err) {
+    static_assert(NPH == ZWS_NPH && sizeof(T) == 4, "k_zws serves FP32 with 9 physical quantities");
+    using V = V2<T>;
+    using Z = ZRCfg<T, N>;
+    constexpr int E = Z::E, SCR = Z::SCR;
+    constexpr unsigned NINV = NPH * 32;   // threads of the inverse warps (named barrier 1)
+    (void)nout;                           // ZWS_NOUT products (the host checks)
+    const int rawf = 2 * ncp;
+    const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tws = reinterpret_cast<V *>(smem_raw);
+    V *lines = tws + Z::LOGE * 32;           // NPH + ZWS_NOUT scratch lines, one per warp
+    V *raw = lines + (NPH + ZWS_NOUT) * SCR;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(raw + NRAW * rawf);
+    T *tkz = reinterpret_cast<T *>(bar + 2);   // kz wavenumbers of the kept modes (ncp entries)
+    __shared__ int stop;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    long long pair = blockIdx.x;
+    if (pair >= npairs) return;   // uniform for the block
+    for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    for (int k = threadIdx.x; k < ncp; k += blockDim.x) tkz[k] = (T)wavenum(k, N, dkz);
+    unsigned keep = 0;   // bit m: mode min(n, N - n) of element n = lane + 32 m is kept
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int n = lane + 32 * m;
+        keep |= ((2 * n <= N ? n : N - n) < nkz ? 1u : 0u) << m;
+    }
+    if (threadIdx.x == 0) {
+        stop = 0;
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](long long p) {
+        mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
+        for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+    };
+    if (threadIdx.x == 0) issue(pair);
+    unsigned parity = 0;
+    const bool inv = warp < NPH;
+    const ZRecipe rc = zr.q[inv ? warp : 0];
+    V *scr = lines + warp * SCR;
+    long long prev = -1;
+    for (;;) {
+        if (inv) {
+            if (pair < npairs) {
+                const bool ok = mbar_wait_bounded(bar, parity);
+                V x[E];
+                zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp,
+                              keep, tkz);
+                if (bar_named_or(1, NINV, !ok)) {   // every inverse warp has unpacked, or one gave up
+                    if (threadIdx.x == 0) {
+                        stop = 1;
+                        mbar_wait_bounded(bar, parity);   // let an overdue copy land before leaving
+                    }
+                } else {
+                    parity ^= 1u;
+                    if (threadIdx.x == 0 && pair + gridDim.x < npairs) {
+                        fence_proxy_async_smem();
+                        issue(pair + gridDim.x);
+                    }
+                    zr_fft<T, N, +1>(lane, x, scr, tws);   // ends its scratch reads with __syncwarp
+#pragma unroll
+                    for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
+                }
+            }
+        } else if (prev >= 0) {   // z R2C of product warp - NPH of the previous pair
+            V x[E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
+            __syncwarp();
+            zr_fft<T, N, -1>(lane, x, scr, tws);
+            zr_store_r2c<T, N>(lane, x, scr, f.p[warp - NPH] + prev * rawf, ncp);
+        }
+        __syncthreads();   // quantities of `pair` in the inverse warps' lines; the forward lines are free
+        if (stop) {
+            if (threadIdx.x == 0) atomicOr(err, 1u);
+            return;
+        }
+        if (pair >= npairs) break;
+        zr_products<T, N, NPH>(lines, lines + NPH * SCR, alpha);
+        __syncthreads();   // products of `pair` in the forward warps' lines
+        prev = pair;
+        pair += gridDim.x;
     }
 }
 

@@ -233,13 +233,18 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  *                          (N = 256, 512) and fit, staged otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
  *                          (N = 256, 512) and fit (a request, not a guarantee);
- *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory.
+ *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory;
+ *   GNSS_VARIANT_WARPSPEC  (GNSS_OPT_ZVARIANT only) the register z kernel
+ *                          with separate inverse and forward warps, where it
+ *                          exists (FP32, one scalar, no colloid term, z
+ *                          length 256 or 512); the register kernel otherwise.
  * Every variant computes the same step to round-off. */
 #define GNSS_OPT_ZVARIANT 0
 #define GNSS_OPT_PVARIANT 1
 #define GNSS_VARIANT_AUTO 0
 #define GNSS_VARIANT_REGISTER 1
 #define GNSS_VARIANT_STAGED 2
+#define GNSS_VARIANT_WARPSPEC 3
 #define GNSS_ZVARIANT_AUTO GNSS_VARIANT_AUTO
 #define GNSS_ZVARIANT_REGISTER GNSS_VARIANT_REGISTER
 #define GNSS_ZVARIANT_STAGED GNSS_VARIANT_STAGED
@@ -286,9 +291,11 @@ gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream);
 long long gnss_ensemble_launches_per_step(const gnss_ensemble *e);
 /* Autotuner: for every member, time each kernel variant (GNSS_OPT_*) over
  * `steps` steps on the member's own buffers (which are zeroed afterwards, so
- * tune before uploading states) and keep the fastest.  Members of equal
- * (grid, precision, scalars, scheme) share one measurement.  choices (may be
- * NULL) receives the chosen GNSS_OPT_ZVARIANT value per member. */
+ * tune before uploading states) and keep the fastest of the z variants
+ * REGISTER, STAGED, WARPSPEC by the pass variants REGISTER, STAGED.  Members
+ * of equal (grid, precision, scalars, scheme, colloid term on/off) share one
+ * measurement.  choices (may be NULL) receives, per member, the chosen
+ * GNSS_OPT_ZVARIANT value + 4 * the GNSS_OPT_PVARIANT value. */
 gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices);
 
 /* ---------------------------------------------------------------- serving

@@ -72,8 +72,9 @@ def test_ensemble_autotune_keeps_results(torch_cuda):
     init = [_init(G, c, seed=3 + i) for i, c in enumerate(cfgs)]
     with G.Ensemble(cfgs, n_branches=2) as ens:
         choices = ens.autotune(2)
-        allowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED)
-        assert all(ch & 3 in allowed and ch >> 2 in allowed for ch in choices)
+        zallowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED, G.GNSS_VARIANT_WARPSPEC)
+        pallowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED)
+        assert all(ch & 3 in zallowed and ch >> 2 in pallowed for ch in choices)
         for i, a in enumerate(init):
             ens.upload(i, a)
         ens.step(4)

@@ -1,7 +1,8 @@
 """The kernel variants of the step give the same step.
 
 At N = 256 and 512 the z stage runs register-resident line transforms
-(k_zreg) and the strided x / y passes register-resident column transforms
+(k_zreg, or k_zws with separate inverse and forward warps in FP32 with one
+scalar) and the strided x / y passes register-resident column transforms
 (k_passr); the staged kernels (k_zphys, k_pass: per-radix-stage transforms
 through shared memory) serve every size.  All evaluate the nonlinear term of
 solver_ps (solver.cu:700-765); here one context steps the same dealiased
@@ -59,7 +60,8 @@ def test_register_and_staged_z_agree(torch_cuda, n, precision, ns, alpha):
     with G.Context(nx=nx, ny=ny, nz=nz, re=3000.0, sc=0.7, sc_c=1.0, alpha=alpha, dt=5e-4, n_scalars=ns,
                    precision=precision) as ctx:
         a = _run(G, torch, ctx, init, 2, A, A)
-        for zv, pv in ((S, A), (A, S), (S, S)):
+        W = G.GNSS_VARIANT_WARPSPEC   # the register kernel where the warp-specialised one does not exist
+        for zv, pv in ((S, A), (A, S), (S, S), (W, A), (W, S)):
             b = _run(G, torch, ctx, init, 2, zv, pv)
             for q in range(3 + ns):
                 err = rel_l2(a[q], b[q])
