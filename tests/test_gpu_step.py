@@ -187,3 +187,5 @@ def test_run_host_matches_device_steps(torch_cuda, shape, scheme, precision, ns,
         h2d, d2h = ctx.run_host_bytes()
         assert d2h == host.numel() * host.element_size()
         assert 0 < h2d < d2h
+        ctx.run_host(host, host, steps, True, None)   # in place, no statistics
+        assert np.array_equal(host.numpy(), out.numpy())
