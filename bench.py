@@ -421,7 +421,7 @@ def ours(args):
         err = run_error_vs_fp64(G, torch, n, args.error_steps, dev)
     ens = None
     if not args.no_ensemble and not args.grid:
-        ens = run_ensemble(G, torch, dev, args.ensemble_steps)
+        ens = run_ensemble(G, torch, dev, args.ensemble_steps, args.ensemble_branches)
         if red is not None:
             ens["value"] = round(ws * ens["points_per_step"] / (red(ens["ms_per_step"]) * 1e-3) / 1e6, 3)
     serve = None
@@ -512,6 +512,7 @@ def main():
     ap.add_argument("--error-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--ensemble-branches", type=int, default=8)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=15.0)
     args = ap.parse_args()
