@@ -234,7 +234,7 @@ def run_error_vs_fp64(G, torch, n, steps, dev) -> dict:
             "max": float(f"{max(errs):.3e}"), "tolerance": 1e-5}
 
 
-# ensemble of BASELINE's batching form: 16 x 64^3, 8 x 96^3, 6 x 128^3, 2 x 192^3
+# the batched ensemble workload: 16 x 64^3, 8 x 96^3, 6 x 128^3, 2 x 192^3
 ENSEMBLE_SIZES = [64] * 16 + [96] * 8 + [128] * 6 + [192] * 2
 
 

@@ -1,7 +1,7 @@
 """Golden initial conditions from the reference's own generator.
 
-    python tests/golden/make_ic_golden.py run [--out DIR]       (on a GPU box)
-    python tests/golden/make_ic_golden.py package [--src DIR]   (anywhere)
+    python tests/golden/make_ic_golden.py run --out DIR        (on a machine with a GPU)
+    python tests/golden/make_ic_golden.py package --src DIR    (anywhere)
 
 `run` executes ``oracle/_ref/<cfg>/refdrv ic`` for the configurations below:
 the reference's initializeJet (initialize.cu:615-641: generateNoise with its
@@ -45,9 +45,11 @@ def package(src: Path) -> None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("step", choices=("run", "package"))
-    ap.add_argument("--out", default=str(ROOT / "gpurun_out" / "ic_golden"))
-    ap.add_argument("--src", default=str(ROOT / "gpurun_out" / "ic_golden"))
+    ap.add_argument("--out", help="directory for the reference's dumps (step run)")
+    ap.add_argument("--src", help="directory holding those dumps (step package)")
     a = ap.parse_args()
+    if (a.out if a.step == "run" else a.src) is None:
+        ap.error("run needs --out, package needs --src")
     if a.step == "run":
         run(Path(a.out))
     else:
