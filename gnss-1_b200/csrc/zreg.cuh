@@ -259,6 +259,72 @@ __device__ __forceinline__ void zr_pack(int lane, V2<T> *x, const ZRecipe rc, co
     }
 }
 
+// The same packing with the recipe fixed at compile time, for the recipes the
+// step uses: sgn[0] = +1 and, with a second term, sgn[1] = -1 (IKZ0, IKZ1:
+// the kz factor on the first, second term; HAS1: a second term).  Same
+// arithmetic as zr_pack in the same order; the keep test is k < nkz, and
+// elements of which no lane is kept are skipped by a warp-uniform test.  The
+// imaginary parts are cleared only where they can be nonzero modes k = 0 and
+// k = N/2, i.e. lane 0 of elements 0 and E/2 (element E/2 uses the upper-half
+// formula at lane 0, which gives the same value once they are cleared).
+template <typename T, int N, bool IKZ0, bool HAS1, bool IKZ1>
+__device__ __forceinline__ void zr_pack_fixed(int lane, V2<T> *x, const V2<T> *a0, const V2<T> *a1, int ncp, int nkz,
+                                              const T *tkz) {
+    using V = V2<T>;
+    constexpr int E = ZRCfg<T, N>::E;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const bool lo = m < E / 2;
+        const int kmin = lo ? 32 * m : N - 31 - 32 * m;   // smallest k of the element over the warp
+        V z = V{T(0), T(0)};
+        if (kmin < nkz) {
+            const int k = lo ? lane + 32 * m : N - lane - 32 * m;
+            if (k < nkz) {
+                V a = a0[k], b = a0[ncp + k];
+                T kz = T(0);
+                if constexpr (IKZ0 || IKZ1) kz = tkz[k];
+                if constexpr (IKZ0) { a = V{-kz * a.y, kz * a.x}; b = V{-kz * b.y, kz * b.x}; }
+                if constexpr (HAS1) {
+                    V c = a1[k], d = a1[ncp + k];
+                    if constexpr (IKZ1) { c = V{-kz * c.y, kz * c.x}; d = V{-kz * d.y, kz * d.x}; }
+                    a = csub(a, c);
+                    b = csub(b, d);
+                }
+                if (m == 0 || m == E / 2) {
+                    if (lane == 0) { a.y = T(0); b.y = T(0); }
+                }
+                z = lo ? V{a.x - b.y, a.y + b.x} : V{a.x + b.y, b.x - a.y};
+            }
+        }
+        x[m] = z;
+    }
+}
+
+// Recipe class for zr_pack_fixed (0 .. 5), or -1 for the general zr_pack.
+__device__ __forceinline__ int zr_kind(const ZRecipe &rc) {
+    if (rc.sgn[0] != 1) return -1;
+    if (rc.r[1] < 0) return rc.ikz[0] ? 1 : 0;
+    if (rc.sgn[1] != -1) return -1;
+    return 2 + (rc.ikz[0] ? 2 : 0) + (rc.ikz[1] ? 1 : 0);
+}
+
+// Packs quantity `rc` of the staged raw line pairs into x (kind = zr_kind(rc)).
+template <typename T, int N>
+__device__ __forceinline__ void zr_pack_any(int kind, int lane, V2<T> *x, const ZRecipe rc, const V2<T> *raw, int rawf,
+                                            int ncp, int nkz, unsigned keep, const T *tkz) {
+    const V2<T> *a0 = raw + rc.r[0] * rawf;
+    const V2<T> *a1 = rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr;
+    switch (kind) {
+        case 0: zr_pack_fixed<T, N, false, false, false>(lane, x, a0, a1, ncp, nkz, tkz); break;
+        case 1: zr_pack_fixed<T, N, true, false, false>(lane, x, a0, a1, ncp, nkz, tkz); break;
+        case 2: zr_pack_fixed<T, N, false, true, false>(lane, x, a0, a1, ncp, nkz, tkz); break;
+        case 3: zr_pack_fixed<T, N, false, true, true>(lane, x, a0, a1, ncp, nkz, tkz); break;
+        case 4: zr_pack_fixed<T, N, true, true, false>(lane, x, a0, a1, ncp, nkz, tkz); break;
+        case 5: zr_pack_fixed<T, N, true, true, true>(lane, x, a0, a1, ncp, nkz, tkz); break;
+        default: zr_pack<T, N>(lane, x, rc, a0, a1, ncp, keep, tkz); break;
+    }
+}
+
 // Pointwise products of one line pair by the whole block: the physical
 // quantities are element pidx(n) of the lines `phys` (stride SCR), product f
 // goes to element pidx(n) of line f of `out` (stride SCR).  out may equal
@@ -369,6 +435,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
     if (threadIdx.x == 0) issue(pair);
     unsigned parity = 0;
     const ZRecipe rc = zr.q[warp];
+    const int kind = zr_kind(rc);
     V *scr = scr_all + warp * SCR;   // transposes, then this warp's physical quantity
     for (; pair < npairs; pair += gridDim.x) {
         const bool ok = mbar_wait_bounded(bar, parity);
@@ -379,8 +446,11 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
         }
         parity ^= 1u;
         V x[E];
-        zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp, keep,
-                      tkz);
+        if constexpr (sizeof(T) == 8)   // measured: faster in FP64; in FP32 the general form keeps 72 registers
+            zr_pack_any<T, N>(kind, lane, x, rc, raw, rawf, ncp, nkz, keep, tkz);
+        else
+            zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp, keep,
+                          tkz);
         __syncthreads();   // staging consumed; the previous pair's products are read
         if (threadIdx.x == 0 && pair + gridDim.x < npairs) {
             fence_proxy_async_smem();
