@@ -116,6 +116,18 @@ def max_over_ranks(x: float) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(x: float) -> float:
+    """Sum of a per-rank scalar over the process group (identity without one)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = f"cuda:{torch.cuda.current_device()}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def replica_value(points: float, ms_max: float, world: int) -> float:
     """Whole-job Mpoint-steps/s: every rank advanced `points` per step in ms_max."""
     return world * points / (ms_max * 1e-3) / 1e6
@@ -428,6 +440,8 @@ def ours(args):
     if not args.no_serve and not args.grid:
         serve = run_serving(G, dev, args.serve_seconds)
         if red is not None:   # whole-job throughput: every rank served its own stream
+            serve["value"] = round(sum_over_ranks(serve["value"]), 3)
+            serve["p50_s"] = red(serve["p50_s"])
             serve["p99_s"] = red(serve["p99_s"])
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

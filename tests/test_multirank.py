@@ -29,7 +29,8 @@ def _rank(rank, world, port, times, out):
     try:
         import bench
         ms = bench.max_over_ranks(times[rank])
-        out[rank] = (ms, bench.replica_value(512.0 ** 3, ms, world))
+        total = bench.sum_over_ranks(times[rank])
+        out[rank] = (ms, bench.replica_value(512.0 ** 3, ms, world), total)
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -48,8 +49,9 @@ def test_two_rank_replicas_take_slowest_rank():
         p.join(timeout=120)
         assert p.exitcode == 0
     for r in range(2):
-        ms, value = out[r]
+        ms, value, total = out[r]
         assert ms == 12.5
+        assert total == 22.5   # the serving leg's whole-job throughput is the sum of the ranks' own
         assert value == pytest.approx(2 * 512.0 ** 3 / 12.5e-3 / 1e6)
 
 
@@ -57,4 +59,5 @@ def test_single_process_is_identity():
     sys.path.insert(0, str(ROOT))
     import bench
     assert bench.max_over_ranks(3.25) == 3.25
+    assert bench.sum_over_ranks(3.25) == 3.25
     assert bench.replica_value(100.0, 1.0, 1) == pytest.approx(0.1)
