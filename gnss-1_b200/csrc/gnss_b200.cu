@@ -171,13 +171,22 @@ template <class K> static int blocks_per_sm(K kern, int threads, int smem) {
     return n < 1 ? 1 : n;
 }
 
+// Line lengths at which GNSS_VARIANT_AUTO takes the register kernels, as
+// measured on B200 in FP32 (ensembles of 16 x 64^3 .. 2 x 192^3 and single
+// jets at 256^3, 512^3): the z kernel at every length it serves; the passes
+// everywhere but N = 64 (16 x 64^3: 6 303 against 7 666 Mpoint-steps/s).
+__host__ __device__ constexpr bool zr_auto_z(int n) { return zr_size(n); }
+__host__ __device__ constexpr bool zr_auto_pass(int n) { return zr_size(n) && n != 64; }
+
 template <typename T, int N> struct Launch {
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
                             cudaStream_t s, int pvariant) {
-        if constexpr (N == 256 || N == 512) {
-            // register-resident column transforms unless staged ones are requested; measured faster
-            // (512^3 FP32 step 7.34 against 8.39 ms, FP64 10.1 against 8.9 Gpoint-steps/s; 256^3 1.23 against 1.28 ms)
-            const bool reg = pvariant != GNSS_VARIANT_STAGED;
+        if constexpr (zr_size(N)) {
+            // register-resident column transforms where they measured faster (512^3 FP32 step 7.34 against
+            // 8.39 ms, FP64 10.1 against 8.9 Gpoint-steps/s; 256^3 1.23 against 1.28 ms; N = 96 .. 192 with
+            // lane shuffles)
+            const bool reg = pvariant == GNSS_VARIANT_REGISTER ||
+                             (pvariant == GNSS_VARIANT_AUTO && zr_auto_pass(N));
             if (reg) {
                 using C = PRCfg<T, N>;
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;
@@ -251,7 +260,7 @@ template <typename T, int N> struct Launch {
     template <int NPH, int NRAW>
     static cudaError_t zreg_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
                               T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s) {
-        if constexpr (N == 256 || N == 512) {
+        if constexpr (zr_size(N)) {
             const int smem = ZRCfg<T, N>::smem_bytes(NPH, NRAW, ncp);
             if (smem > ZPCfg<T, N>::SMEM_MAX) return cudaErrorNotSupported;
             auto kern = k_zreg<T, N, NPH, NRAW>;
@@ -300,7 +309,7 @@ template <typename T, int N> struct Launch {
             return false;
     }
     static bool zreg_fits(int nph, int nraw, int ncp) {
-        if constexpr (N == 256 || N == 512)
+        if constexpr (zr_size(N))
             return ZRCfg<T, N>::smem_bytes(nph, nraw, ncp) <= ZPCfg<T, N>::SMEM_MAX;
         else
             return false;
@@ -310,7 +319,9 @@ template <typename T, int N> struct Launch {
                              unsigned *err, int nsm, cudaStream_t s, int zvariant) {
         if (zvariant == GNSS_VARIANT_WARPSPEC && zws_fits(nph, nraw, nout, ncp))
             return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
-        if (zvariant != GNSS_VARIANT_STAGED && zreg_fits(nph, nraw, ncp)) {
+        const bool reg = zvariant == GNSS_VARIANT_REGISTER || zvariant == GNSS_VARIANT_WARPSPEC ||
+                         (zvariant == GNSS_VARIANT_AUTO && zr_auto_z(N));
+        if (reg && zreg_fits(nph, nraw, ncp)) {
             if (nph == 9 && nraw == 10)
                 return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
             if (nph == 12 && nraw == 13)

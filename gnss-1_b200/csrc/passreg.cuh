@@ -68,7 +68,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     const long long nitems = (long long)sp.nin * ntiles;
     long long item = blockIdx.x;
     if (item >= nitems) return;
-    for (int i = tid; i < Z::LOGE * 32; i += NT) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    for (int i = tid; i < Z::LOGE * 32; i += NT) tws[i] = tw[Z::tw_index(i)];
     auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
         fi = (int)(it / ntiles);
         const int t = (int)(it % ntiles);

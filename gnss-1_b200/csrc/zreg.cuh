@@ -87,17 +87,38 @@ template <int S, typename V> struct Dft<16, S, V> {
     static __device__ __forceinline__ void run(V *v) { dft16<S>(v); }
 };
 
+// Line lengths the register transforms serve: N = 32 E with E = 8, 16 (one
+// transpose through shared memory, zr_fft) or E = 2, 3, 4, 6 (lane shuffles
+// only, zs_fft).
+__host__ __device__ constexpr bool zr_size(int n) {
+    return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 512;
+}
+
 template <typename T, int N> struct ZRCfg {
+    static_assert(zr_size(N), "register transforms serve N = 64, 96, 128, 192, 256, 512");
     static constexpr int E = N / 32;                    // elements per lane
-    static constexpr int G = 32 / E;                    // lanes per group in step B
+    static constexpr bool SHFL = E != 8 && E != 16;     // lane-shuffle scheme (no transpose)
+    static constexpr int G = SHFL ? 1 : 32 / E;         // lanes per group in step B (transpose scheme)
     static constexpr int S = 32 + G;                    // transpose row stride (conflict-free both ways)
-    static constexpr int SCR = E * S;                   // transpose scratch per warp
-    static constexpr int LOGE = E == 16 ? 4 : 3;        // table powers W^(lane 2^b), b < LOGE
-    static constexpr int PADP = (sizeof(T) == 4 && E == 8) ? 8 : 0;   // line padding per 64 entries
-    static constexpr int PL = N + PADP * (N / 64);      // physical line length in shared memory
-    __host__ __device__ static constexpr int pidx(int n) { return n + PADP * (n >> 6); }
-    static_assert(E == 8 || E == 16, "register z transform serves N = 256 and 512");
+    // table rows: W^(lane 2^b), b < LOGE (transpose scheme); W_N^(lane k1) for
+    // k1 = 1 .. E-1, then W_32^lane (shuffle scheme)
+    static constexpr int LOGE = SHFL ? E : (E == 16 ? 4 : 3);
+    // line padding: per 64 entries (transpose scheme, FP32 E = 8); in the
+    // shuffle scheme c entries per E, so that a warp's stores of one output
+    // element (positions q + E j, j = 0 .. 31) fall in distinct bank pairs
+    static constexpr int PADP = (sizeof(T) == 4 && E == 8) ? 8 : 0;
+    static constexpr int PADC = SHFL ? ((E & 1) ? 2 : 1) : 0;
+    __host__ __device__ static constexpr int pidx(int n) {
+        return SHFL ? n + PADC * (n / E) : n + PADP * (n >> 6);
+    }
+    static constexpr int PL = SHFL ? N + PADC * 32 : N + PADP * (N / 64);   // line length in shared memory
+    static constexpr int SCR = SHFL ? PL : E * S;       // scratch line per warp (transposes, physical line)
     static_assert(SCR >= PL, "scratch holds a padded line");
+    // index into the length-N table exp(-2 pi i j / N) of twiddle-table entry i
+    __host__ __device__ static constexpr int tw_index(int i) {
+        const int row = i >> 5, l = i & 31;
+        return SHFL ? (row < E - 1 ? (l * (row + 1)) % N : (E * l) % N) : ((l << row) % N);
+    }
     // twiddle powers, scratch lines (one per warp; they also hold the physical
     // lines and the products), raw staging, mbarrier (16 B), kz table (ncp T)
     __host__ __device__ static constexpr int smem_bytes(int nph, int nraw, int ncp) {
@@ -106,6 +127,26 @@ template <typename T, int N> struct ZRCfg {
     // k_zws: one more scratch line per forward warp
     __host__ __device__ static constexpr int smem_bytes_ws(int nph, int nout, int nraw, int ncp) {
         return smem_bytes(nph + nout, nraw, ncp);
+    }
+};
+
+// 6-point DFT in natural order: n = 2 n1 + n2, k = k1 + 3 k2 (two 3-point
+// DFTs, twiddles W_6^(n2 k1), one 2-point stage).
+template <int S, typename V> struct Dft<6, S, V> {
+    static __device__ __forceinline__ void run(V *v) {
+        using T = decltype(v[0].x);
+        const T h = T(0.5);
+        const T s3 = T(S) * T(0.86602540378443864676372317075294);
+        V a[3] = {v[0], v[2], v[4]}, b[3] = {v[1], v[3], v[5]};
+        Dft<3, S, V>::run(a);
+        Dft<3, S, V>::run(b);
+        b[1] = V{h * b[1].x - s3 * b[1].y, h * b[1].y + s3 * b[1].x};     // W_6^1 = 1/2 + i S sqrt(3)/2
+        b[2] = V{-h * b[2].x - s3 * b[2].y, -h * b[2].y + s3 * b[2].x};   // W_6^2 = -1/2 + i S sqrt(3)/2
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+            v[k1] = cadd(a[k1], b[k1]);
+            v[k1 + 3] = csub(a[k1], b[k1]);
+        }
     }
 };
 
@@ -147,6 +188,43 @@ template <typename T, int N> struct ZrScratch {
     __device__ __forceinline__ int operator()(int k1, int i) const { return k1 * ZRCfg<T, N>::S + i; }
 };
 
+// Length-N DFT (N = 32 E, E = 2, 3, 4, 6) of one line held by a warp, with
+// lane shuffles only.  On entry x[m] is element lane + 32 m; on return x[q]
+// is element q + E bitrev5(lane) of the transform.  n = lane + 32 m,
+// k = k1 + E k2: an E-point DFT over m in registers, the twiddle
+// W_N^(lane k1), then for every k1 a 32-point DFT across the lanes in five
+// radix-2 decimation-in-frequency steps (partner lane ^ h: p + s x with s = +1
+// on the lower and -1 on the upper lane, the upper one then multiplied by
+// W_{2h}^(lane mod h)).  tws rows: W_N^(lane k1), k1 = 1 .. E-1, then W_32^lane
+// (exp(-2 pi i ./.), conjugated for SIGN > 0).
+template <typename T, int N, int SIGN>
+__device__ __forceinline__ void zs_fft(int lane, V2<T> *x, const V2<T> *tws) {
+    using V = V2<T>;
+    constexpr int E = N / 32;
+    auto tw_at = [&](int i) {
+        V t = tws[i];
+        if (SIGN > 0) t.y = -t.y;
+        return t;
+    };
+    Dft<E, SIGN, V>::run(x);
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) x[k1] = cmul(x[k1], tw_at(32 * (k1 - 1) + lane));
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool upper = (lane & h) != 0;
+        const T sg = upper ? T(-1) : T(1);
+        V w = V{T(1), T(0)};
+        if (h > 1 && upper) w = tw_at(32 * (E - 1) + (lane & (h - 1)) * (16 / h));
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const V p = shfl_xor_v(x[q], h);
+            V t = V{p.x + sg * x[q].x, p.y + sg * x[q].y};
+            if (h > 1) t = cmul(t, w);
+            x[q] = t;
+        }
+    }
+}
+
 // Length-N DFT of one line held by a warp.  On entry x[m] is element
 // lane + 32 m; on return x[q] is element k1 + E q + E^2 zr_sigma(j) of the
 // transform, with k1 = lane / G, j = lane % G.  The one transpose goes
@@ -157,6 +235,12 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
     constexpr int E = Z::E, G = Z::G;
+    if constexpr (Z::SHFL) {   // N = 64, 96, 128, 192: no transpose
+        (void)scr;
+        (void)at;
+        zs_fft<T, N, SIGN>(lane, x, tws);
+        return;
+    } else {
     Dft<E, SIGN, V>::run(x);
     {
         // W^k1 for k1 = 1, 2, 4 (, 8) from the table, the others as products
@@ -218,12 +302,16 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
             x[q] = V{p2.x + s0 * c.x, p2.y + s0 * c.y};
         }
     }
+    }
 }
 
 // Line index held in x[q] after zr_fft.
 template <typename T, int N> __device__ __forceinline__ int zr_out_index(int lane, int q) {
     using Z = ZRCfg<T, N>;
-    return lane / Z::G + Z::E * q + Z::E * Z::E * zr_sigma<Z::G>(lane % Z::G);
+    if constexpr (Z::SHFL)
+        return q + Z::E * (int)(__brev((unsigned)lane) >> 27);
+    else
+        return lane / Z::G + Z::E * q + Z::E * Z::E * zr_sigma<Z::G>(lane % Z::G);
 }
 
 // C2R packing (as pack_c2r_combo) straight into the registers of zr_fft:
@@ -415,7 +503,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     long long pair = blockIdx.x;
     if (pair >= npairs) return;   // uniform for the block
-    for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[Z::tw_index(i)];
     for (int k = threadIdx.x; k < ncp; k += blockDim.x) tkz[k] = (T)wavenum(k, N, dkz);
     unsigned keep = 0;   // bit m: mode min(n, N - n) of element n = lane + 32 m is kept
 #pragma unroll
@@ -446,7 +534,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
         }
         parity ^= 1u;
         V x[E];
-        if constexpr (sizeof(T) == 8)   // measured: faster in FP64; in FP32 the general form keeps 72 registers
+        if constexpr (sizeof(T) == 8 && E % 2 == 0)   // measured: faster in FP64; in FP32 the general form keeps 72 registers
             zr_pack_any<T, N>(kind, lane, x, rc, raw, rawf, ncp, nkz, keep, tkz);
         else
             zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp, keep,
@@ -507,7 +595,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     long long pair = blockIdx.x;
     if (pair >= npairs) return;   // uniform for the block
-    for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[((i & 31) << (i >> 5)) % N];
+    for (int i = threadIdx.x; i < Z::LOGE * 32; i += blockDim.x) tws[i] = tw[Z::tw_index(i)];
     for (int k = threadIdx.x; k < ncp; k += blockDim.x) tkz[k] = (T)wavenum(k, N, dkz);
     unsigned keep = 0;   // bit m: mode min(n, N - n) of element n = lane + 32 m is kept
 #pragma unroll

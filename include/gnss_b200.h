@@ -229,10 +229,13 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  * the kernel of the strided x and y passes (of the step and of the 3D
  * transforms):
  *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
- *                          resident line transforms where they exist
- *                          (N = 256, 512) and fit, staged otherwise;
+ *                          resident transforms where they fit (z: every N
+ *                          below; x / y passes: all of them but N = 64),
+ *                          staged otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
- *                          (N = 256, 512) and fit (a request, not a guarantee);
+ *                          (N = 64, 96, 128, 192 with lane shuffles only;
+ *                          N = 256, 512 with one transpose) and fit (a
+ *                          request, not a guarantee);
  *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory;
  *   GNSS_VARIANT_WARPSPEC  (GNSS_OPT_ZVARIANT only) the register z kernel
  *                          with separate inverse and forward warps, where it

@@ -3,13 +3,14 @@
 At N = 256 and 512 the z stage runs register-resident line transforms
 (k_zreg, or k_zws with separate inverse and forward warps in FP32 with one
 scalar) and the strided x / y passes register-resident column transforms
-(k_passr); the staged kernels (k_zphys, k_pass: per-radix-stage transforms
-through shared memory) serve every size.  All evaluate the nonlinear term of
+(k_passr); at N = 64, 96, 128 and 192 the same kernels run lane-shuffle
+transforms when requested; the staged kernels (k_zphys, k_pass:
+per-radix-stage transforms through shared memory) serve every size.  All evaluate the nonlinear term of
 solver_ps (solver.cu:700-765); here one context steps the same dealiased
 state with every combination of the two options (gnss_set_option) and the
 fields must agree to round-off: relative L2 <= 1e-13 in FP64 and <= 2e-6 in
 FP32 after two steps.  The FP64 register path is also held to the oracle at
-256^3 (1e-12 after one step).
+256^3, 96^3 and 128^3 (1e-12 after one step).
 """
 import numpy as np
 import pytest
@@ -25,6 +26,13 @@ CASES = [
     (512, 1, 1, 0.0),
     ((64, 64, 512), 0, 2, 0.05),   # z length 512: forward transforms split in halves, 5 products
     ((64, 64, 512), 1, 1, 0.0),
+    # lane-shuffle register transforms (N = 32 E, E = 2, 3, 4, 6)
+    (64, 0, 2, 0.05),
+    (96, 1, 1, 0.0),
+    (128, 0, 1, 0.0),
+    (192, 1, 2, 0.0),
+    ((96, 64, 192), 0, 1, 0.0),
+    ((128, 192, 64), 1, 2, 0.05),
 ]
 
 
@@ -69,11 +77,14 @@ def test_register_and_staged_z_agree(torch_cuda, n, precision, ns, alpha):
 
 
 @pytest.mark.gpu
-def test_register_z_matches_oracle_256(torch_cuda, oracle):
+@pytest.mark.parametrize("n", [256, 96, 128])
+def test_register_z_matches_oracle(torch_cuda, oracle, n):
+    """FP64 register kernels (both z and passes) against the oracle after one step: the default (AUTO)
+    selection at 256, the lane-shuffle transforms requested explicitly at 96 and 128."""
     import gnss_b200 as G
     torch = torch_cuda
-    n, ns = 256, 2
-    init = G.jet_initial_state(n, n_scalars=ns, seed=11, noise_kmax=16.0, amp=0.05)
+    ns = 2
+    init = G.jet_initial_state(n, n_scalars=ns, seed=11, noise_kmax=min(16.0, n / 8), amp=0.05)
     oc = oracle.cfg(n, re=3000.0, sc=0.7, sc_c=1.0, dt=5e-4)
     f = [x.copy() for x in init]
     r = [np.zeros_like(init[0]) for _ in range(5)]
@@ -82,14 +93,15 @@ def test_register_z_matches_oracle_256(torch_cuda, oracle):
     oracle.step_cnab2(oc, f, r, euler=True)
     with G.Context(n, re=3000.0, sc=0.7, sc_c=1.0, dt=5e-4, n_scalars=ns) as ctx:
         assert ctx.get_option(G.GNSS_OPT_ZVARIANT) == G.GNSS_ZVARIANT_AUTO
-        got = _run(G, torch, ctx, init, 1, G.GNSS_ZVARIANT_AUTO)
+        v = G.GNSS_VARIANT_AUTO if n == 256 else G.GNSS_VARIANT_REGISTER
+        got = _run(G, torch, ctx, init, 1, v, v)
     for q in range(3 + ns):
         err = rel_l2(got[q], f[q])
         assert err < 1e-12, f"field {q}: rel L2 {err:.3e}"
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(256, 256, 32), (512, 8, 16), (16, 512, 8)])
+@pytest.mark.parametrize("shape", [(256, 256, 32), (512, 8, 16), (16, 512, 8), (64, 96, 16), (192, 128, 8)])
 def test_register_passes_in_the_3d_transforms(torch_cuda, oracle, shape):
     """gnss_forward / gnss_inverse (fftfuncs.cu:288-359) with the register pass kernel, against the oracle."""
     import gnss_b200 as G
