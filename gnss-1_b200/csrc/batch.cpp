@@ -299,6 +299,9 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
             if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, zv)) ||
                 (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, pv)))
                 break;
+            int zk = 0;
+            if (zv == GNSS_VARIANT_WARPSPEC && (gnss_get_option(mb.ctx, GNSS_OPT_ZKERNEL, &zk) || zk != zv))
+                continue;   // no warp-specialised kernel here: the same kernels as the register choice
             if ((st = gnss_step(mb.ctx, &mb.state, &mb.hist, 1, bs))) break;   // warm-up
             cudaEventRecord(t0, bs);
             for (int i = 0; i < steps && !st; ++i) st = gnss_step(mb.ctx, &mb.state, &mb.hist, 0, bs);

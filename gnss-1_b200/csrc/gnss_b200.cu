@@ -314,14 +314,20 @@ template <typename T, int N> struct Launch {
         else
             return false;
     }
+    // the z kernel a variant option selects: GNSS_VARIANT_WARPSPEC, _REGISTER or _STAGED
+    static int zkernel(int zvariant, int nph, int nraw, int nout, int ncp) {
+        if (zvariant == GNSS_VARIANT_WARPSPEC && zws_fits(nph, nraw, nout, ncp)) return GNSS_VARIANT_WARPSPEC;
+        const bool reg = zvariant == GNSS_VARIANT_REGISTER || zvariant == GNSS_VARIANT_WARPSPEC ||
+                         (zvariant == GNSS_VARIANT_AUTO && zr_auto_z(N));
+        return reg && zreg_fits(nph, nraw, ncp) ? GNSS_VARIANT_REGISTER : GNSS_VARIANT_STAGED;
+    }
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
                              unsigned *err, int nsm, cudaStream_t s, int zvariant) {
-        if (zvariant == GNSS_VARIANT_WARPSPEC && zws_fits(nph, nraw, nout, ncp))
+        const int kern = zkernel(zvariant, nph, nraw, nout, ncp);
+        if (kern == GNSS_VARIANT_WARPSPEC)
             return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
-        const bool reg = zvariant == GNSS_VARIANT_REGISTER || zvariant == GNSS_VARIANT_WARPSPEC ||
-                         (zvariant == GNSS_VARIANT_AUTO && zr_auto_z(N));
-        if (reg && zreg_fits(nph, nraw, ncp)) {
+        if (kern == GNSS_VARIANT_REGISTER) {
             if (nph == 9 && nraw == 10)
                 return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
             if (nph == 12 && nraw == 13)
@@ -340,7 +346,8 @@ template <typename T, int N> struct Launch {
     }
 };
 
-#define GNSS_SIZE_SWITCH(n, EXPR)                   \
+#define GNSS_SIZE_SWITCH(n, EXPR) GNSS_SIZE_SWITCH_OR(n, EXPR, return cudaErrorInvalidValue)
+#define GNSS_SIZE_SWITCH_OR(n, EXPR, DEFAULT)       \
     switch (n) {                                    \
         case 8: { constexpr int NN_ = 8; EXPR; }    \
         case 12: { constexpr int NN_ = 12; EXPR; }  \
@@ -355,7 +362,7 @@ template <typename T, int N> struct Launch {
         case 256: { constexpr int NN_ = 256; EXPR; } \
         case 384: { constexpr int NN_ = 384; EXPR; } \
         case 512: { constexpr int NN_ = 512; EXPR; } \
-        default: return cudaErrorInvalidValue;      \
+        default: DEFAULT;                           \
     }
 
 template <typename T>
@@ -888,10 +895,18 @@ gnss_status gnss_set_option(gnss_ctx *c, int key, int value) {
     return GNSS_OK;
 }
 
+template <typename T> static int zkernel_of(const gnss_ctx *c) {
+    GNSS_SIZE_SWITCH_OR(c->g.nz,
+                        return (Launch<T, NN_>::zkernel(c->zvariant, c->n_phys, c->n_raw, c->nnl, c->ncp)),
+                        return GNSS_VARIANT_STAGED);
+}
+
 gnss_status gnss_get_option(const gnss_ctx *c, int key, int *value) {
     if (!c || !value) return GNSS_ERR_INVALID;
     if (key == GNSS_OPT_ZVARIANT) *value = c->zvariant;
     else if (key == GNSS_OPT_PVARIANT) *value = c->pvariant;
+    else if (key == GNSS_OPT_ZKERNEL)
+        *value = c->cfg.precision == GNSS_FP64 ? zkernel_of<double>(c) : zkernel_of<float>(c);
     else return GNSS_ERR_INVALID;
     return GNSS_OK;
 }

@@ -34,6 +34,7 @@ GNSS_FP32 = 1
 GNSS_NSTATS = 7
 GNSS_OPT_ZVARIANT = 0
 GNSS_OPT_PVARIANT = 1
+GNSS_OPT_ZKERNEL = 2   # read-only: the z kernel the options select
 GNSS_VARIANT_AUTO = GNSS_ZVARIANT_AUTO = 0
 GNSS_VARIANT_REGISTER = GNSS_ZVARIANT_REGISTER = 1
 GNSS_VARIANT_STAGED = GNSS_ZVARIANT_STAGED = 2

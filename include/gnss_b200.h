@@ -244,6 +244,8 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  * Every variant computes the same step to round-off. */
 #define GNSS_OPT_ZVARIANT 0
 #define GNSS_OPT_PVARIANT 1
+#define GNSS_OPT_ZKERNEL 2   /* read-only (gnss_get_option): the z kernel the options select for this
+                              * context, GNSS_VARIANT_WARPSPEC, _REGISTER or _STAGED */
 #define GNSS_VARIANT_AUTO 0
 #define GNSS_VARIANT_REGISTER 1
 #define GNSS_VARIANT_STAGED 2

@@ -122,3 +122,27 @@ def test_register_passes_in_the_3d_transforms(torch_cuda, oracle, shape):
         ctx.inverse_transform(t)
         torch.cuda.synchronize()
         assert rel_max(buffer_to_phys(to_host(t), shape), u) < 1e-13
+
+
+@pytest.mark.gpu
+def test_z_kernel_query(torch_cuda):
+    """GNSS_OPT_ZKERNEL reports the z kernel the options select (read-only)."""
+    import gnss_b200 as G
+    W, R, S, A = G.GNSS_VARIANT_WARPSPEC, G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED, G.GNSS_VARIANT_AUTO
+    cases = [
+        # config, z option -> kernel
+        (dict(n=256, precision=G.GNSS_FP32), W, W),
+        (dict(n=256, precision=G.GNSS_FP64), W, R),      # warp-specialised kernel: FP32 only
+        (dict(n=256, precision=G.GNSS_FP32, n_scalars=2), W, R),
+        (dict(n=128, precision=G.GNSS_FP32), W, R),      # and z length 256 or 512 only
+        (dict(n=128, precision=G.GNSS_FP32), A, R),
+        (dict(n=128, precision=G.GNSS_FP32), S, S),
+        (dict(n=48, precision=G.GNSS_FP32), R, S),       # no register transform of length 48
+    ]
+    for kw, opt, want in cases:
+        n = kw.pop("n")
+        with G.Context(n, **kw) as ctx:
+            ctx.set_option(G.GNSS_OPT_ZVARIANT, opt)
+            assert ctx.get_option(G.GNSS_OPT_ZKERNEL) == want, (n, kw, opt)
+            with pytest.raises(G.GnssError):
+                ctx.set_option(G.GNSS_OPT_ZKERNEL, R)
