@@ -172,11 +172,15 @@ template <class K> static int blocks_per_sm(K kern, int threads, int smem) {
 }
 
 // Line lengths at which GNSS_VARIANT_AUTO takes the register kernels, as
-// measured on B200 in FP32 (ensembles of 16 x 64^3 .. 2 x 192^3 and single
-// jets at 256^3, 512^3): the z kernel at every length it serves; the passes
-// everywhere but N = 64 (16 x 64^3: 6 303 against 7 666 Mpoint-steps/s).
+// measured on B200 (ensembles of 16 x 64^3 .. 2 x 192^3 and single jets at
+// 256^3, 512^3): the z kernel at every length it serves; the passes at
+// N = 96 .. 512 in FP32 (at N = 64 the staged pass: 8 931 against 7 759
+// Mpoint-steps/s for 16 x 64^3) and at N = 256, 512 in FP64 (below, staged:
+// 7 542 against 6 743 for 2 x 192^3).
 __host__ __device__ constexpr bool zr_auto_z(int n) { return zr_size(n); }
-__host__ __device__ constexpr bool zr_auto_pass(int n) { return zr_size(n) && n != 64; }
+__host__ __device__ constexpr bool zr_auto_pass(int n, bool fp64) {
+    return zr_size(n) && (fp64 ? n >= 256 : n != 64);
+}
 
 template <typename T, int N> struct Launch {
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
@@ -186,7 +190,7 @@ template <typename T, int N> struct Launch {
             // 8.39 ms, FP64 10.1 against 8.9 Gpoint-steps/s; 256^3 1.23 against 1.28 ms; N = 96 .. 192 with
             // lane shuffles)
             const bool reg = pvariant == GNSS_VARIANT_REGISTER ||
-                             (pvariant == GNSS_VARIANT_AUTO && zr_auto_pass(N));
+                             (pvariant == GNSS_VARIANT_AUTO && zr_auto_pass(N, sizeof(T) == 8));
             if (reg) {
                 using C = PRCfg<T, N>;
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;

@@ -52,7 +52,7 @@ template <typename T, int N> struct ColScratch {
 template <int N> __device__ __forceinline__ int row_dist(int r) { return r <= N / 2 ? r : N - r; }
 
 template <typename T, int N, int SIGN>
-__global__ void __launch_bounds__(PRCfg<T, N>::NT, 1)
+__global__ void __launch_bounds__(PRCfg<T, N>::NT, (N <= 192 && sizeof(T) == 4) ? 2 : 1)
 k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec sp, const V2<T> *__restrict__ tw) {
     using V = V2<T>;
     using C = PRCfg<T, N>;

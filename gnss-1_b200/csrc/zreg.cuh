@@ -486,7 +486,7 @@ __device__ __forceinline__ void zr_store_r2c(int lane, const V2<T> *x, V2<T> *sc
 // cp.async.bulk (CTA-local, no multicast) while the current pair is
 // processed; a wait that times out sets bit 0 of *err and the block stops.
 template <typename T, int N, int NPH, int NRAW>
-__global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? 3 : 1)
+__global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? (N <= 192 ? 4 : 3) : (N <= 192 ? 2 : 1))
 k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
        int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err) {
     using V = V2<T>;

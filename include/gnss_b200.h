@@ -230,8 +230,8 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  * transforms):
  *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
  *                          resident transforms where they fit (z: every N
- *                          below; x / y passes: all of them but N = 64),
- *                          staged otherwise;
+ *                          below; x / y passes: N = 96 .. 512 in FP32,
+ *                          256 and 512 in FP64), staged otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
  *                          (N = 64, 96, 128, 192 with lane shuffles only;
  *                          N = 256, 512 with one transpose) and fit (a
