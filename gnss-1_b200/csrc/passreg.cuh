@@ -48,6 +48,18 @@ template <typename T, int N> struct ColScratch {
     }
 };
 
+// Row of the output tile that holds transform row r.  With lane shuffles a
+// lane ends holding rows q + E j (j = bitrev5(lane)); storing row q + E j at
+// tile row 32 q + j makes a warp's stores of one q land in distinct bank
+// pairs (row r itself would put 32 / E lanes on each, with the pitch LD).
+template <typename T, int N> __device__ __forceinline__ int pr_tile_row(int r) {
+    using Z = ZRCfg<T, N>;
+    if constexpr (Z::SHFL)
+        return (r % Z::E) * 32 + r / Z::E;
+    else
+        return r;
+}
+
 // |row index| of a transform row (the Nyquist row counts as N/2)
 template <int N> __device__ __forceinline__ int row_dist(int r) { return r <= N / 2 ? r : N - r; }
 
@@ -153,8 +165,14 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                 }
             }
             zr_fft<T, N, SIGN>(lane, x, col, tws, ColScratch<T, N>{});
+            if constexpr (Z::SHFL) {
+                const int j = (int)(__brev((unsigned)lane) >> 27);
 #pragma unroll
-            for (int q = 0; q < E; ++q) col[zr_out_index<T, N>(lane, q) * LD] = x[q];
+                for (int q = 0; q < E; ++q) col[(32 * q + j) * LD] = x[q];   // pr_tile_row(q + E j)
+            } else {
+#pragma unroll
+                for (int q = 0; q < E; ++q) col[zr_out_index<T, N>(lane, q) * LD] = x[q];
+            }
             __syncthreads();   // output tile complete
             V *dst = P.out[sp.vout[fi][v]] + dbase + tid % NB;
             if (tid % NB < out_cols) {
@@ -164,7 +182,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                 for (int rc = tid / NB; rc < nrow; rc += RSTEP) {
                     const int row = sp.row_out.expand(rc);
                     const int r = sp.row_out_compact ? rc : row;
-                    dst[r * drow] = src[row * LD];
+                    dst[r * drow] = src[pr_tile_row<T, N>(row) * LD];
                 }
             }
             if (v + 1 < nv) __syncthreads();   // output tile free for the next output
