@@ -260,7 +260,7 @@ template <typename T, int N> struct Launch {
             return zphys_k<NPH, NRAW, true>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
         return zphys_k<NPH, NRAW, false>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
     }
-    // register-resident line transforms (N = 256, 512) when their shared memory fits
+    // register-resident line transforms (N = 64 .. 512, zr_size) when their shared memory fits
     template <int NPH, int NRAW>
     static cudaError_t zreg_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
                               T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s) {

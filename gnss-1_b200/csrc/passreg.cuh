@@ -1,5 +1,5 @@
 // passreg.cuh -- strided x / y passes with register-resident column
-// transforms (N = 256, 512).
+// transforms (N = 64, 96, 128, 192, 256, 512).
 //
 // Same contract as k_pass (PassSpec / PassPtrs: tiles of NB columns x N rows,
 // kept / compact rows and outer indices, up to two outputs per tile, each the

@@ -1,17 +1,19 @@
-// zreg.cuh -- fused z pass with register-resident line transforms (N = 256, 512).
+// zreg.cuh -- fused z pass with register-resident line transforms
+// (N = 64, 96, 128, 192, 256, 512).
 //
 // Same work as k_zphys (kz factors and vorticity combinations, C2R of every
 // physical quantity of a line pair, the pointwise products, R2C of the
 // products), with a different line transform: a warp holds its line in
-// registers, E = N/32 elements per lane, and runs the length-N DFT as
+// registers, E = N/32 elements per lane.  For N = 64 .. 192 (E = 2, 3, 4, 6)
+// the transform uses lane shuffles only (zs_fft).  For N = 256, 512 it runs
 //   N = E * 32,   32 = E * G   (G = 32/E lanes per group)
 //   step A: E-point DFT in registers over elements lane + 32 m, twiddle
 //           W_N^(lane k1);
 //   one transpose through a padded per-warp scratch;
 //   step B: E-point DFT in registers, twiddle W_32^(j k2'), and a G-point
 //           DFT across the lanes of a group with shuffles.
-// A line therefore crosses shared memory once per transform (instead of once
-// per radix-8 stage), the C2R packing is done while loading the registers,
+// so a line crosses shared memory once per transform (instead of once per
+// radix-8 stage).  The C2R packing is done while loading the registers,
 // and the twiddles of step A are products of four table powers.  Each warp
 // leaves its physical quantity in its own scratch line, where the other warps
 // read it; the whole block forms the products in place, into the lines of the
