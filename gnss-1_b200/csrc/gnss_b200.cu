@@ -261,25 +261,28 @@ template <typename T, int N> struct Launch {
         return zphys_k<NPH, NRAW, false>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
     }
     // register-resident line transforms (N = 64 .. 512, zr_size) when their shared memory fits
+    // diag != nullptr: the instantiation that also writes per-block vorticity sums there
     template <int NPH, int NRAW>
     static cudaError_t zreg_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
-                              T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s) {
+                              T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s,
+                              double *diag = nullptr) {
         if constexpr (zr_size(N)) {
             const int smem = ZRCfg<T, N>::smem_bytes(NPH, NRAW, ncp);
             if (smem > ZPCfg<T, N>::SMEM_MAX) return cudaErrorNotSupported;
-            auto kern = k_zreg<T, N, NPH, NRAW>;
+            auto kern = diag ? k_zreg<T, N, NPH, NRAW, true> : k_zreg<T, N, NPH, NRAW, false>;
             cudaError_t e = prep_smem(kern, smem);
             if (e != cudaSuccess) return e;
             const int per_sm = blocks_per_sm(kern, NPH * 32, smem);
             const long long npairs = nlines / 2;
             long long grid = (long long)per_sm * nsm;
             if (grid > npairs) grid = npairs;
+            if (diag && grid > STAT_BLOCKS) grid = STAT_BLOCKS;   // one row of sums per block
             kern<<<(unsigned)grid, NPH * 32, smem, s>>>(f, zr, nout, npairs, ncp, nkz, scale, alpha, dkz,
-                                                         reinterpret_cast<const V2<T> *>(tw), err);
+                                                         reinterpret_cast<const V2<T> *>(tw), err, diag);
             return cudaGetLastError();
         } else {
             (void)f; (void)zr; (void)nout; (void)nlines; (void)ncp; (void)nkz; (void)scale; (void)alpha; (void)dkz;
-            (void)tw; (void)err; (void)nsm; (void)s;
+            (void)tw; (void)err; (void)nsm; (void)s; (void)diag;
             return cudaErrorNotSupported;
         }
     }
@@ -325,9 +328,21 @@ template <typename T, int N> struct Launch {
                          (zvariant == GNSS_VARIANT_AUTO && zr_auto_z(N));
         return reg && zreg_fits(nph, nraw, ncp) ? GNSS_VARIANT_REGISTER : GNSS_VARIANT_STAGED;
     }
+    // diag != nullptr: the register kernel with the fused vorticity sums (cudaErrorNotSupported where it does
+    // not exist)
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
-                             unsigned *err, int nsm, cudaStream_t s, int zvariant) {
+                             unsigned *err, int nsm, cudaStream_t s, int zvariant, double *diag = nullptr) {
+        if (diag) {
+            if (!zreg_fits(nph, nraw, ncp)) return cudaErrorNotSupported;
+            if (nph == 9 && nraw == 10)
+                return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag);
+            if (nph == 12 && nraw == 13)
+                return zreg_k<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag);
+            if (nph == 14 && nraw == 14)
+                return zreg_k<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag);
+            return cudaErrorInvalidValue;
+        }
         const int kern = zkernel(zvariant, nph, nraw, nout, ncp);
         if (kern == GNSS_VARIANT_WARPSPEC)
             return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
@@ -382,10 +397,11 @@ static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfield
 template <typename T>
 static cudaError_t launch_zphys(int n, const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                                 long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
-                                unsigned *err, int nsm, cudaStream_t s, int zvariant) {
+                                unsigned *err, int nsm, cudaStream_t s, int zvariant, double *diag = nullptr) {
     GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::zphys(f, zr, nph, nraw, nout, nlines, ncp, nkz, scale, alpha, dkz, tw,
-                                                      err, nsm, s, zvariant)));
+                                                      err, nsm, s, zvariant, diag)));
 }
+
 template <typename T> static int pass_nb(int n) {
     switch (n) {
         case 8: return PassCfg<T, 8>::NB; case 12: return PassCfg<T, 12>::NB;
@@ -595,7 +611,8 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
 //   6 projection, dealias and time update                                  (P, state, hist)
 template <typename T>
 static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, void *hist_base, const gnss_fields *hist,
-                                        const UpdCoef &uc, cudaStream_t s, double *stats_dst = nullptr) {
+                                        const UpdCoef &uc, cudaStream_t s, double *stats_dst = nullptr,
+                                        double *diag = nullptr) {
     const Geom &g = c->g;
     const int np = c->n_xout, nq = c->n_raw, nnl = c->nnl;
     gnss_status st = ensure_scratch_step(c);
@@ -645,7 +662,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
     {
         StageTimer t(c, s, 2);
         CK(c, launch_zphys<T>(g.nz, Q, c->zrec, c->n_phys, nq, nnl, nlines, c->ncp, c->nkz, scale, (T)c->cfg.alpha,
-                              g.dkz, c->tw[2], c->d_err, c->nsm, s, c->zvariant));
+                              g.dkz, c->tw[2], c->d_err, c->nsm, s, c->zvariant, diag));
     }
     {
         StageTimer t(c, s, 3);
@@ -707,11 +724,11 @@ static UpdCoef base_coef(const gnss_ctx *c) {
 
 template <typename T>
 static gnss_status step_t(gnss_ctx *c, const gnss_fields *state, const gnss_fields *hist, int euler, cudaStream_t s,
-                          double *stats_dst = nullptr) {
+                          double *stats_dst = nullptr, double *diag = nullptr) {
     UpdCoef uc = base_coef(c);
     if (c->cfg.scheme == GNSS_SCHEME_CNAB2) {
         uc.euler = euler ? 1 : 0;
-        return nonlinear_and_update<T>(c, state, nullptr, hist, uc, s, stats_dst);
+        return nonlinear_and_update<T>(c, state, nullptr, hist, uc, s, stats_dst, diag);
     }
     // IF-RK3: the history lives in context scratch after the step's quantities
     gnss_status st = ensure_scratch_step(c);
@@ -725,7 +742,8 @@ static gnss_status step_t(gnss_ctx *c, const gnss_fields *state, const gnss_fiel
         uc.gam = gam[k];
         uc.zet_next = zet[k + 1];
         uc.alph = gam[k] + zet[k];
-        st = nonlinear_and_update<T>(c, state, hb, nullptr, uc, s, k == 2 ? stats_dst : nullptr);
+        st = nonlinear_and_update<T>(c, state, hb, nullptr, uc, s, k == 2 ? stats_dst : nullptr,
+                                     k == 0 ? diag : nullptr);   // the state the step starts from
         if (st) return st;
     }
     return GNSS_OK;
@@ -771,10 +789,8 @@ static void stats_of_sums(const gnss_ctx *c, const double *h, double *out) {
 // statistics over the grid after three inverse transforms of the vorticity
 // (scratch fields 1..3; field 0 is the transforms' own scratch); mean
 // profiles from the kx = kz = 0 modes.
-template <typename T>
-static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *out, double *yprof, cudaStream_t s) {
-    const Geom &g = c->g;
-    const size_t nvals = TURB_SUMS + VORT_SUMS + 5 * (size_t)g.ny;
+static gnss_status ensure_turb_buffers(gnss_ctx *c) {
+    const size_t nvals = TURB_SUMS + VORT_SUMS + 5 * (size_t)c->g.ny;
     if (!c->turb_part) {
         if (cudaMalloc(&c->turb_part, sizeof(double) * STAT_BLOCKS * std::max(TURB_SUMS, VORT_SUMS)) != cudaSuccess ||
             cudaMalloc(&c->turb_dev, sizeof(double) * nvals) != cudaSuccess ||
@@ -784,16 +800,28 @@ static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *o
         }
         c->owned_bytes += sizeof(double) * (STAT_BLOCKS * std::max(TURB_SUMS, VORT_SUMS) + nvals);
     }
-    gnss_status stt = ensure_scratch(c, 4);
-    if (stt) return stt;
-    FieldSet<T> F{};
-    void *sp[5] = {st->u, st->v, st->w, st->s, st->c};
-    for (int q = 0; q < 5; ++q) F.p[q] = reinterpret_cast<V2<T> *>(sp[q]);
-    c->launches += 2;
-    k_turb_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(F, st->s != nullptr, g, c->turb_part);
+    return GNSS_OK;
+}
+
+// spectral sums and mean profiles of a state into turb_dev (no synchronisation)
+template <typename T> static gnss_status turb_spectral_t(gnss_ctx *c, const FieldSet<T> &F, bool has_s, cudaStream_t s) {
+    const Geom &g = c->g;
+    c->launches += 3;
+    k_turb_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(F, has_s, g, c->turb_part);
     LAUNCH_CK(c);
     k_sums_final<TURB_SUMS><<<1, TURB_SUMS * 32, 0, s>>>(c->turb_part, STAT_BLOCKS, TURB_SUMS, c->turb_dev);
     LAUNCH_CK(c);
+    k_yprof<T><<<5, 256, 0, s>>>(F, g, reinterpret_cast<const V2<T> *>(c->tw[1]),
+                                 c->turb_dev + TURB_SUMS + VORT_SUMS);
+    LAUNCH_CK(c);
+    return GNSS_OK;
+}
+
+// vorticity sums over the grid into turb_dev + TURB_SUMS, by three inverse transforms (no synchronisation)
+template <typename T> static gnss_status turb_vort_t(gnss_ctx *c, const FieldSet<T> &F, cudaStream_t s) {
+    const Geom &g = c->g;
+    gnss_status stt = ensure_scratch(c, 4);
+    if (stt) return stt;
     V2<T> *o[3];
     for (int q = 0; q < 3; ++q) o[q] = fld<T>(c->scratch, c->nspec, 1 + q);
     c->launches++;
@@ -803,7 +831,7 @@ static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *o
         gnss_status e = inverse_t<T>(c, o[q], s);
         if (e) return e;
     }
-    c->launches += 3;
+    c->launches += 2;
     k_vort_partial<T><<<STAT_BLOCKS, STAT_THREADS, 0, s>>>(reinterpret_cast<const T *>(o[0]),
                                                             reinterpret_cast<const T *>(o[1]),
                                                             reinterpret_cast<const T *>(o[2]), g, c->turb_part);
@@ -811,9 +839,13 @@ static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *o
     k_sums_final<VORT_SUMS><<<1, VORT_SUMS * 32, 0, s>>>(c->turb_part, STAT_BLOCKS, VORT_SUMS,
                                                          c->turb_dev + TURB_SUMS);
     LAUNCH_CK(c);
-    k_yprof<T><<<5, 256, 0, s>>>(F, g, reinterpret_cast<const V2<T> *>(c->tw[1]),
-                                 c->turb_dev + TURB_SUMS + VORT_SUMS);
-    LAUNCH_CK(c);
+    return GNSS_OK;
+}
+
+// turb_dev to the host and into gnss_turb (synchronises)
+static gnss_status turb_finish(gnss_ctx *c, bool has_s, gnss_turb *out, double *yprof, cudaStream_t s) {
+    const Geom &g = c->g;
+    const size_t nvals = TURB_SUMS + VORT_SUMS + 5 * (size_t)g.ny;
     CK(c, cudaMemcpyAsync(c->turb_host, c->turb_dev, sizeof(double) * nvals, cudaMemcpyDeviceToHost, s));
     CK(c, cudaStreamSynchronize(s));
     gnss_status chk = gnss_check(c, s);
@@ -827,13 +859,61 @@ static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *o
     out->eta = std::sqrt(std::sqrt(nu * nu * nu / out->epsilon));
     out->l = 3 * M_PI / 4 * (h[2] / n2) / out->ke;
     out->lambda = std::sqrt(15.0 * nu * out->vrms * out->vrms / out->epsilon);
-    out->chi = st->s ? 2.0 * (nu / k.sc) * (h[3] / n2) : 0.0;
+    out->chi = has_s ? 2.0 * (nu / k.sc) * (h[3] / n2) : 0.0;
     out->omega = h[TURB_SUMS] / nn;
     out->omega_x = std::sqrt(h[TURB_SUMS + 1] / nn);
     out->omega_y = std::sqrt(h[TURB_SUMS + 2] / nn);
     out->omega_z = std::sqrt(h[TURB_SUMS + 3] / nn);
     if (yprof) std::memcpy(yprof, h + TURB_SUMS + VORT_SUMS, sizeof(double) * 5 * (size_t)g.ny);
     return GNSS_OK;
+}
+
+template <typename T> static FieldSet<T> fieldset_of(const gnss_fields *st) {
+    FieldSet<T> F{};
+    void *sp[5] = {st->u, st->v, st->w, st->s, st->c};
+    for (int q = 0; q < 5; ++q) F.p[q] = reinterpret_cast<V2<T> *>(sp[q]);
+    return F;
+}
+
+template <typename T>
+static gnss_status turb_stats_t(gnss_ctx *c, const gnss_fields *st, gnss_turb *out, double *yprof, cudaStream_t s) {
+    gnss_status r = ensure_turb_buffers(c);
+    if (r) return r;
+    const FieldSet<T> F = fieldset_of<T>(st);
+    if ((r = turb_spectral_t<T>(c, F, st->s != nullptr, s))) return r;
+    if ((r = turb_vort_t<T>(c, F, s))) return r;
+    return turb_finish(c, st->s != nullptr, out, yprof, s);
+}
+
+template <typename T> static bool zdiag_fits(const gnss_ctx *c) {
+    GNSS_SIZE_SWITCH_OR(c->g.nz, return (Launch<T, NN_>::zreg_fits(c->n_phys, c->n_raw, c->ncp)), return false);
+}
+
+// One step with the calcTurbStats statistics of the state it starts from.  The
+// spectral sums and profiles come from that state before the step; the
+// vorticity sums from the physical vorticity the step's z kernel forms anyway
+// (per-block rows into turb_part, zeroed first, summed after the step), where a
+// register z kernel exists; elsewhere from three inverse transforms of the
+// vorticity before the step.
+template <typename T>
+static gnss_status step_turb_t(gnss_ctx *c, const gnss_fields *st, const gnss_fields *hist, int euler, gnss_turb *out,
+                               double *yprof, cudaStream_t s) {
+    gnss_status r = ensure_turb_buffers(c);
+    if (r) return r;
+    const FieldSet<T> F = fieldset_of<T>(st);
+    if ((r = turb_spectral_t<T>(c, F, st->s != nullptr, s))) return r;
+    if (zdiag_fits<T>(c)) {
+        CK(c, cudaMemsetAsync(c->turb_part, 0, sizeof(double) * STAT_BLOCKS * VORT_SUMS, s));
+        if ((r = step_t<T>(c, st, hist, euler, s, nullptr, c->turb_part))) return r;
+        c->launches++;
+        k_sums_final<VORT_SUMS><<<1, VORT_SUMS * 32, 0, s>>>(c->turb_part, STAT_BLOCKS, VORT_SUMS,
+                                                             c->turb_dev + TURB_SUMS);
+        LAUNCH_CK(c);
+    } else {
+        if ((r = turb_vort_t<T>(c, F, s))) return r;
+        if ((r = step_t<T>(c, st, hist, euler, s))) return r;
+    }
+    return turb_finish(c, st->s != nullptr, out, yprof, s);
 }
 
 // ============================================================== C ABI
@@ -1414,6 +1494,17 @@ gnss_status gnss_step(gnss_ctx *c, const gnss_fields *state, const gnss_fields *
     if (!al_fields(c, state) || !al_fields(c, hist)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
     CK(c, cudaSetDevice(c->cfg.device));
     return PREC_CALL(c, step_t, c, state, hist, euler, S(stream));
+}
+
+gnss_status gnss_step_turb(gnss_ctx *c, const gnss_fields *state, const gnss_fields *hist, int euler, gnss_turb *out,
+                           double *yprof, void *stream) {
+    if (!c || !out) return fail(c, GNSS_ERR_INVALID, "null argument");
+    if (!state_ok(c, state)) return fail(c, GNSS_ERR_INVALID, "state fields missing");
+    if (c->cfg.scheme == GNSS_SCHEME_CNAB2 && !state_ok(c, hist))
+        return fail(c, GNSS_ERR_INVALID, "history fields missing");
+    if (!al_fields(c, state) || !al_fields(c, hist)) return fail(c, GNSS_ERR_INVALID, "misaligned pointer");
+    CK(c, cudaSetDevice(c->cfg.device));
+    return PREC_CALL(c, step_turb_t, c, state, hist, euler, out, yprof, S(stream));
 }
 
 gnss_status gnss_stats(gnss_ctx *c, const gnss_fields *state, double *out, void *stream) {

@@ -426,8 +426,13 @@ __device__ __forceinline__ void zr_pack_any(int kind, int lane, V2<T> *x, const 
 // zphys_products: (w x u) (crossProductKernel_mgpu, solver.cu:139-164),
 // u . grad s (dotKernel_mgpu, solver.cu:342-356) and the colloid term
 // (colloidAdvectionKernel_mgpu, solver.cu:374-388).
-template <typename T, int N, int NPH>
-__device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alpha) {
+// With DIAG, the thread also adds to acc the vorticity sums of its points
+// (ZR_VORT_SUMS: |w|, w_x^2, w_y^2, w_z^2, both lines of the pair), the sums
+// of k_vort_partial (statistics.cu:1211-1305), from the physical quantities 3,
+// 4, 5 = w_x, w_y, w_z it reads anyway.
+constexpr int ZR_VORT_SUMS = 4;
+template <typename T, int N, int NPH, bool DIAG = false>
+__device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alpha, double *acc = nullptr) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
     constexpr int SCR = Z::SCR;
@@ -438,6 +443,13 @@ __device__ __forceinline__ void zr_products(const V2<T> *phys, V2<T> *out, T alp
         const V u = p[0 * SCR], v = p[1 * SCR], w = p[2 * SCR];
         const V o1 = p[3 * SCR], o2 = p[4 * SCR], o3 = p[5 * SCR];
         const V sx = p[6 * SCR], sy = p[7 * SCR], sz = p[8 * SCR];
+        if constexpr (DIAG) {
+            const double ax = o1.x, ay = o2.x, az = o3.x, bx = o1.y, by = o2.y, bz = o3.y;
+            acc[0] += sqrt(ax * ax + ay * ay + az * az) + sqrt(bx * bx + by * by + bz * bz);
+            acc[1] += ax * ax + bx * bx;
+            acc[2] += ay * ay + by * by;
+            acc[3] += az * az + bz * bz;
+        }
         V *o = out + pn;
         o[0 * SCR] = V{o2.x * w.x - o3.x * v.x, o2.y * w.y - o3.y * v.y};
         o[1 * SCR] = V{-o1.x * w.x + o3.x * u.x, -o1.y * w.y + o3.y * u.y};
@@ -487,13 +499,18 @@ __device__ __forceinline__ void zr_store_r2c(int lane, const V2<T> *x, V2<T> *sc
 // physical quantity q.  The raw lines of the next pair arrive by
 // cp.async.bulk (CTA-local, no multicast) while the current pair is
 // processed; a wait that times out sets bit 0 of *err and the block stops.
-template <typename T, int N, int NPH, int NRAW>
+// With DIAG the block also writes one row of ZR_VORT_SUMS vorticity sums over
+// its points to diag[blockIdx.x] (fixed-order reduction), for the statistics
+// of the state the step starts from.
+template <typename T, int N, int NPH, int NRAW, bool DIAG = false>
 __global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? (N <= 192 ? 4 : 3) : (N <= 192 ? 2 : 1))
 k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
-       int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err) {
+       int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err,
+       double *__restrict__ diag = nullptr) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
     constexpr int E = Z::E, SCR = Z::SCR;
+    double acc[DIAG ? ZR_VORT_SUMS : 1] = {};
     const int rawf = 2 * ncp;
     const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -550,7 +567,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
 #pragma unroll
         for (int q = 0; q < E; ++q) scr[Z::pidx(zr_out_index<T, N>(lane, q))] = cscale(x[q], scale);
         __syncthreads();   // every physical quantity on chip
-        zr_products<T, N, NPH>(scr_all, scr_all, alpha);
+        zr_products<T, N, NPH, DIAG>(scr_all, scr_all, alpha, acc);
         __syncthreads();   // products in the scratch lines of warps 0 .. nout-1
         if (warp < nout) {   // z R2C of product `warp`, written over raw field `warp` of the pair
 #pragma unroll
@@ -558,6 +575,21 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
             __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
             zr_store_r2c<T, N>(lane, x, scr, f.p[warp] + pair * rawf, ncp);
+        }
+    }
+    if constexpr (DIAG) {   // warp shuffles, then the block's warps in order
+        __shared__ double red[ZR_VORT_SUMS][NPH];
+#pragma unroll
+        for (int q = 0; q < ZR_VORT_SUMS; ++q) {
+            double v = acc[q];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) red[q][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < ZR_VORT_SUMS) {
+            double v = 0.0;
+            for (int w = 0; w < NPH; ++w) v += red[threadIdx.x][w];
+            diag[blockIdx.x * ZR_VORT_SUMS + threadIdx.x] = v;
         }
     }
 }

@@ -126,6 +126,8 @@ _SIGS = {
     "gnss_checkpoint_load": [_VP, ctypes.c_char_p, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields),
                              ctypes.POINTER(ctypes.c_longlong), _VP],
     "gnss_turb_stats": [_VP, ctypes.POINTER(GnssFields), _VP, ctypes.POINTER(ctypes.c_double), _VP],
+    "gnss_step_turb": [_VP, ctypes.POINTER(GnssFields), ctypes.POINTER(GnssFields), ctypes.c_int, _VP,
+                       ctypes.POINTER(ctypes.c_double), _VP],
     "gnss_attach_scratch": [_VP, _VP, ctypes.c_size_t],
     "gnss_ensemble_create": [ctypes.POINTER(GnssConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
     "gnss_ensemble_destroy": [_VP],
@@ -404,6 +406,19 @@ class Context:
         f = _fields(state)
         self._ck(self.lib.gnss_turb_stats(self._h, ctypes.byref(f), ctypes.byref(t), pp, _stream(stream)),
                  "gnss_turb_stats")
+        d = {k: getattr(t, k) for k, _ in GnssTurb._fields_}
+        d["lambda"] = d.pop("lambda_")
+        return d, prof
+
+    def step_turb(self, state: Sequence, hist: Sequence | None, euler: bool, profiles: bool = True, stream=None):
+        """One step plus turb_stats of the state it starts from; the vorticity statistics are summed by the
+        step's own z kernel where the register kernel serves the context."""
+        t = GnssTurb()
+        prof = np.zeros((5, self.cfg.ny)) if profiles else None
+        pp = prof.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if prof is not None else None
+        h = _fields(hist)
+        self._ck(self.lib.gnss_step_turb(self._h, ctypes.byref(_fields(state)), ctypes.byref(h) if h else None,
+                                         int(bool(euler)), ctypes.byref(t), pp, _stream(stream)), "gnss_step_turb")
         d = {k: getattr(t, k) for k, _ in GnssTurb._fields_}
         d["lambda"] = d.pop("lambda_")
         return d, prof

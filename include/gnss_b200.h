@@ -177,6 +177,18 @@ typedef struct gnss_turb {
 } gnss_turb;
 gnss_status gnss_turb_stats(gnss_ctx *ctx, const gnss_fields *state, gnss_turb *out, double *yprof, void *stream);
 
+/* gnss_step (solver_ps, solver.cu:700-765) together with gnss_turb_stats of
+ * the state the step starts from (calcTurbStats_mgpu, statistics.cu:2039-2156,
+ * which the reference calls on the state between steps).  Where the register
+ * z kernel serves the context, the vorticity statistics are summed by the
+ * step's own z kernel from the physical vorticity it forms for the nonlinear
+ * term, so they cost no transforms; elsewhere they come from three inverse
+ * transforms before the step, as in gnss_turb_stats.  For a dealiased state
+ * (the precondition of the step) the statistics equal gnss_turb_stats to
+ * round-off and the new state equals gnss_step's.  Synchronises the stream. */
+gnss_status gnss_step_turb(gnss_ctx *ctx, const gnss_fields *state, const gnss_fields *hist, int euler,
+                           gnss_turb *out, double *yprof, void *stream);
+
 /* End-to-end call with host buffers: copies the packed host state
  * (3 + n_scalars spectral fields back to back) to context-owned device
  * buffers, dealiases it (main.cu:156), runs n_steps steps (the first one

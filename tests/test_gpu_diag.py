@@ -68,3 +68,60 @@ def test_turb_stats_of_taylor_green(torch_cuda):
     m = np.mean(np.abs(2 * np.sin(X[:, :, 0]) * np.sin(Y[:, :, 0])))
     assert math.isclose(got["omega"], m, rel_tol=1e-12)
     assert np.abs(prof).max() < 1e-15
+
+
+STEP_TURB_CASES = [
+    # shape, n_scalars, precision, alpha, scheme
+    ((128, 128, 128), 2, 0, 0.0, 0),   # register z kernel: vorticity sums fused into the step
+    ((96, 96, 96), 1, 1, 0.0, 0),
+    ((64, 64, 64), 2, 1, 0.05, 0),     # colloid term (14 physical quantities)
+    ((64, 48, 64), 1, 1, 0.0, 1),      # IF-RK3: the first substep sees the state the step starts from
+    ((48, 32, 24), 1, 0, 0.0, 0),      # staged z kernel: vorticity by transforms before the step
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,ns,precision,alpha,scheme", STEP_TURB_CASES,
+                         ids=[f"{'x'.join(map(str, c[0]))}_s{c[1]}_{'fp64' if c[2] == 0 else 'fp32'}"
+                              f"{'_alpha' if c[3] else ''}{'_rk3' if c[4] else ''}" for c in STEP_TURB_CASES])
+def test_step_turb_matches_separate_calls(torch_cuda, shape, ns, precision, alpha, scheme):
+    """gnss_step_turb = gnss_turb_stats of the state before the step + gnss_step.
+
+    Spectral statistics and profiles come from the same kernels (equal); the
+    vorticity statistics from the step's own physical vorticity where the
+    register z kernel serves (1e-10 relative in FP64, 2e-5 in FP32); the new
+    state as gnss_step's (1e-14 / 1e-6 relative L2)."""
+    import gnss_b200 as G
+    from _util import rel_l2, to_host
+    torch = torch_cuda
+    nx, ny, nz = shape
+    cdt = np.complex128 if precision == 0 else np.complex64
+    f = [a.astype(cdt) for a in G.jet_initial_state(nx, ny, nz, n_scalars=ns, seed=4, noise_kmax=6.0, amp=0.08)]
+    tol = 1e-10 if precision == 0 else 2e-5
+    stol = 1e-14 if precision == 0 else 1e-6
+    with G.Context(nx=nx, ny=ny, nz=nz, re=1500.0, sc=0.7, sc_c=1.0, alpha=alpha, dt=1e-3, n_scalars=ns,
+                   precision=precision, scheme=scheme) as ctx:
+        runs = []
+        for fused in (False, True):
+            st = [to_dev(torch, a) for a in f]
+            hi = [torch.zeros_like(st[0]) for _ in st]
+            ctx.de_alias(st)
+            for step in range(2):   # two steps in a row (Euler, then AB2)
+                if fused:
+                    got, prof = ctx.step_turb(st, hi, euler=(step == 0))
+                else:
+                    got, prof = ctx.turb_stats(st)
+                    ctx.solver_ps(st, hi, euler=(step == 0))
+                runs.append((got, prof))
+            torch.cuda.synchronize()
+            runs.append([to_host(t) for t in st])
+    sep, fus = runs[:3], runs[3:]
+    for step in range(2):
+        (a, pa), (b, pb) = sep[step], fus[step]
+        for k in ("vrms", "ke", "epsilon", "eta", "l", "lambda", "chi"):
+            assert a[k] == b[k], (step, k)
+        assert np.array_equal(pa, pb)
+        for k in ("omega", "omega_x", "omega_y", "omega_z"):
+            assert math.isclose(a[k], b[k], rel_tol=tol), (step, k, a[k], b[k])
+    for q in range(3 + ns):
+        assert rel_l2(fus[2][q], sep[2][q]) <= stol, q
