@@ -102,9 +102,14 @@ template <typename T, int N> struct ZRCfg {
     static constexpr bool SHFL = E != 8 && E != 16;     // lane-shuffle scheme (no transpose)
     static constexpr int G = SHFL ? 1 : 32 / E;         // lanes per group in step B (transpose scheme)
     static constexpr int S = 32 + G;                    // transpose row stride (conflict-free both ways)
-    // table rows: W^(lane 2^b), b < LOGE (transpose scheme); W_N^(lane k1) for
-    // k1 = 1 .. E-1, then W_32^lane (shuffle scheme)
-    static constexpr int LOGE = SHFL ? E : (E == 16 ? 4 : 3);
+    // table rows: the transpose scheme reads its step-A twiddles W_N^(lane k1)
+    // from the table in FP32 (row k1 - 1, k1 = 1 .. E-1; TWFULL) and builds
+    // them from the powers W^(lane 2^b), b < LOGE, in FP64 (measured: FP32
+    // step 7.15 -> 7.08 ms, FP64 12.80 -> 12.90 ms with the full table at
+    // 512^3); the shuffle scheme reads W_N^(lane k1), k1 = 1 .. E-1, then
+    // W_32^lane
+    static constexpr bool TWFULL = !SHFL && sizeof(T) == 4;
+    static constexpr int LOGE = (SHFL || TWFULL) ? E : (E == 16 ? 4 : 3);
     // line padding: per 64 entries (transpose scheme, FP32 E = 8); in the
     // shuffle scheme c entries per E, so that a warp's stores of one output
     // element (positions q + E j, j = 0 .. 31) fall in distinct bank pairs
@@ -119,7 +124,8 @@ template <typename T, int N> struct ZRCfg {
     // index into the length-N table exp(-2 pi i j / N) of twiddle-table entry i
     __host__ __device__ static constexpr int tw_index(int i) {
         const int row = i >> 5, l = i & 31;
-        return SHFL ? (row < E - 1 ? (l * (row + 1)) % N : (E * l) % N) : ((l << row) % N);
+        return SHFL ? (row < E - 1 ? (l * (row + 1)) % N : (E * l) % N)
+                    : (TWFULL ? (l * (row + 1)) % N : (l << row) % N);
     }
     // twiddle powers, scratch lines (one per warp; they also hold the physical
     // lines and the products), raw staging, mbarrier (16 B), kz table (ncp T)
@@ -231,7 +237,7 @@ __device__ __forceinline__ void zs_fft(int lane, V2<T> *x, const V2<T> *tws) {
 // lane + 32 m; on return x[q] is element k1 + E q + E^2 zr_sigma(j) of the
 // transform, with k1 = lane / G, j = lane % G.  The one transpose goes
 // through scr at offsets at(k1, i) (row k1 = 0..E-1, entry i = 0..31);
-// tws: table powers tws[32 b + l] = exp(-2 pi i l 2^b / N).
+// tws: the twiddle table of ZRCfg (rows tw_index).
 template <typename T, int N, int SIGN, class AT = ZrScratch<T, N>>
 __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<T> *tws, AT at = AT{}) {
     using V = V2<T>;
@@ -245,34 +251,43 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
     } else {
     Dft<E, SIGN, V>::run(x);
     {
-        // W^k1 for k1 = 1, 2, 4 (, 8) from the table, the others as products
-        // (w3 = w1 w2, w5 = w1 w4, w6 = w2 w4, w7 = w3 w4, w(8+i) = w(i) w8),
-        // each applied as soon as it is formed
-        auto tw_at = [&](int b) {
-            V t = tws[32 * b + lane];
-            if (SIGN > 0) t.y = -t.y;
-            return t;
-        };
-        const V w1 = tw_at(0), w2 = tw_at(1), w4 = tw_at(2);
-        const V w3 = cmul(w1, w2);
-        if constexpr (E == 16) {
-            const V w8 = tw_at(3);
-            x[8] = cmul(x[8], w8);
-            x[9] = cmul(x[9], cmul(w1, w8));
-            x[10] = cmul(x[10], cmul(w2, w8));
-            x[11] = cmul(x[11], cmul(w3, w8));
-            x[12] = cmul(x[12], cmul(w4, w8));
-            x[13] = cmul(x[13], cmul(cmul(w1, w4), w8));
-            x[14] = cmul(x[14], cmul(cmul(w2, w4), w8));
-            x[15] = cmul(x[15], cmul(cmul(w3, w4), w8));
+        if constexpr (Z::TWFULL) {   // every W^(lane k1) from the table
+#pragma unroll
+            for (int k1 = 1; k1 < E; ++k1) {
+                V t = tws[32 * (k1 - 1) + lane];
+                if (SIGN > 0) t.y = -t.y;
+                x[k1] = cmul(x[k1], t);
+            }
+        } else {
+            // W^k1 for k1 = 1, 2, 4 (, 8) from the table, the others as products
+            // (w3 = w1 w2, w5 = w1 w4, w6 = w2 w4, w7 = w3 w4, w(8+i) = w(i) w8),
+            // each applied as soon as it is formed
+            auto tw_at = [&](int b) {
+                V t = tws[32 * b + lane];
+                if (SIGN > 0) t.y = -t.y;
+                return t;
+            };
+            const V w1 = tw_at(0), w2 = tw_at(1), w4 = tw_at(2);
+            const V w3 = cmul(w1, w2);
+            if constexpr (E == 16) {
+                const V w8 = tw_at(3);
+                x[8] = cmul(x[8], w8);
+                x[9] = cmul(x[9], cmul(w1, w8));
+                x[10] = cmul(x[10], cmul(w2, w8));
+                x[11] = cmul(x[11], cmul(w3, w8));
+                x[12] = cmul(x[12], cmul(w4, w8));
+                x[13] = cmul(x[13], cmul(cmul(w1, w4), w8));
+                x[14] = cmul(x[14], cmul(cmul(w2, w4), w8));
+                x[15] = cmul(x[15], cmul(cmul(w3, w4), w8));
+            }
+            x[1] = cmul(x[1], w1);
+            x[2] = cmul(x[2], w2);
+            x[3] = cmul(x[3], w3);
+            x[4] = cmul(x[4], w4);
+            x[5] = cmul(x[5], cmul(w1, w4));
+            x[6] = cmul(x[6], cmul(w2, w4));
+            x[7] = cmul(x[7], cmul(w3, w4));
         }
-        x[1] = cmul(x[1], w1);
-        x[2] = cmul(x[2], w2);
-        x[3] = cmul(x[3], w3);
-        x[4] = cmul(x[4], w4);
-        x[5] = cmul(x[5], cmul(w1, w4));
-        x[6] = cmul(x[6], cmul(w2, w4));
-        x[7] = cmul(x[7], cmul(w3, w4));
     }
 #pragma unroll
     for (int k1 = 0; k1 < E; ++k1) scr[at(k1, lane)] = x[k1];
