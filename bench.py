@@ -321,7 +321,7 @@ def run_serving(G, dev, duration_s=15.0, rate=4.0) -> dict:
     budget = 150 << 30
     # untimed warm-up on a server of its own: one short request per (size, scalars), so that the timed stream
     # does not pay the first launch of each kernel
-    with G.Server(budget_bytes=budget, max_active=64, steps_per_launch=25, device=dev) as srv:
+    with G.Server(budget_bytes=budget, max_active=16, steps_per_launch=25, device=dev) as srv:
         wids = [srv.submit(G.make_config(n, re=1000.0, sc=0.7, sc_c=1.0, dt=5e-4, n_scalars=ns,
                                          precision=G.GNSS_FP32, device=dev), st, 26)
                 for (n, ns), st in pool.items()]
@@ -329,7 +329,7 @@ def run_serving(G, dev, duration_s=15.0, rate=4.0) -> dict:
             srv.wait(rid, timeout=600.0)
             srv.result(rid)
     ids = []
-    with G.Server(budget_bytes=budget, max_active=64, steps_per_launch=25, device=dev) as srv:
+    with G.Server(budget_bytes=budget, max_active=16, steps_per_launch=25, device=dev) as srv:
         t0 = time.perf_counter()
         for a, cfg, st, steps in reqs:
             d = t0 + a - time.perf_counter()
@@ -352,7 +352,7 @@ def run_serving(G, dev, duration_s=15.0, rate=4.0) -> dict:
             "completed": rep["completed"], "failed": rep["failed"], "active_max": rep["active_max"],
             "budget_gb": budget / 2 ** 30, "reserved_max_gb": round(rep["bytes_reserved_max"] / 2 ** 30, 2),
             "workload": "Poisson arrivals, N in {64,96,128,192,256}^3, Re ~ U[500,5000], 100-2000 steps, "
-                        "1-2 scalars, FP32, dt 5e-4; 25 steps per graph launch, 64 slots, 150 GB budget; "
+                        "1-2 scalars, FP32, dt 5e-4; 25 steps per graph launch, 16 slots, 150 GB budget; "
                         "after an untimed warm-up request per (size, scalars)"}
 
 
