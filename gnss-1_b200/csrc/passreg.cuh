@@ -33,7 +33,8 @@ template <typename T, int N> struct PRCfg {
     static constexpr int LD = NB + 1;                     // padded row
     static constexpr int TILE = N * LD;
     // two input tiles (the copy pipeline) and one output tile
-    static constexpr int SMEM = (3 * TILE + Z::LOGE * 32) * (int)sizeof(V2<T>);
+    static constexpr int TWR = Z::rows(true);            // twiddle rows (the full step-A table in FP32)
+    static constexpr int SMEM = (3 * TILE + TWR * 32) * (int)sizeof(V2<T>);
 };
 
 // zr_fft's transpose inside the warp's own column of the output tile: row k1
@@ -80,7 +81,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     const long long nitems = (long long)sp.nin * ntiles;
     long long item = blockIdx.x;
     if (item >= nitems) return;
-    for (int i = tid; i < Z::LOGE * 32; i += NT) tws[i] = tw[Z::tw_index(i)];
+    for (int i = tid; i < C::TWR * 32; i += NT) tws[i] = tw[Z::tw_index(i, true)];
     auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
         fi = (int)(it / ntiles);
         const int t = (int)(it % ntiles);
@@ -164,7 +165,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                     x[m] = V{-k2 * x[m].x, -k2 * x[m].y};
                 }
             }
-            zr_fft<T, N, SIGN>(lane, x, col, tws, ColScratch<T, N>{});
+            zr_fft<T, N, SIGN, ColScratch<T, N>, true>(lane, x, col, tws, ColScratch<T, N>{});
             if constexpr (Z::SHFL) {
                 const int j = (int)(__brev((unsigned)lane) >> 27);
 #pragma unroll

@@ -102,14 +102,20 @@ template <typename T, int N> struct ZRCfg {
     static constexpr bool SHFL = E != 8 && E != 16;     // lane-shuffle scheme (no transpose)
     static constexpr int G = SHFL ? 1 : 32 / E;         // lanes per group in step B (transpose scheme)
     static constexpr int S = 32 + G;                    // transpose row stride (conflict-free both ways)
-    // table rows: the transpose scheme reads its step-A twiddles W_N^(lane k1)
-    // from the table in FP32 (row k1 - 1, k1 = 1 .. E-1; TWFULL) and builds
-    // them from the powers W^(lane 2^b), b < LOGE, in FP64 (measured: FP32
-    // step 7.15 -> 7.08 ms, FP64 12.80 -> 12.90 ms with the full table at
-    // 512^3); the shuffle scheme reads W_N^(lane k1), k1 = 1 .. E-1, then
+    // table rows: in the FP32 passes the transpose scheme reads its step-A
+    // twiddles W_N^(lane k1) from the table (row k1 - 1, k1 = 1 .. E-1;
+    // TWFULL); the z kernels and FP64 build them from the powers
+    // W^(lane 2^b), b < LOGE (measured at 512^3 with the full table: FP32
+    // passes 0.06 ms faster per step, the z kernel 0.02 ms slower, FP64 0.1 ms
+    // slower); the shuffle scheme reads W_N^(lane k1), k1 = 1 .. E-1, then
     // W_32^lane
     static constexpr bool TWFULL = !SHFL && sizeof(T) == 4;
-    static constexpr int LOGE = (SHFL || TWFULL) ? E : (E == 16 ? 4 : 3);
+    // rows of the table with (full, where TWFULL) or without the full step-A twiddles; the z kernels use the
+    // powers (their shared-memory traffic is the tighter limit), the passes the full table
+    __host__ __device__ static constexpr int rows(bool full) {
+        return (SHFL || (full && TWFULL)) ? E : (E == 16 ? 4 : 3);
+    }
+    static constexpr int LOGE = rows(false);
     // line padding: per 64 entries (transpose scheme, FP32 E = 8); in the
     // shuffle scheme c entries per E, so that a warp's stores of one output
     // element (positions q + E j, j = 0 .. 31) fall in distinct bank pairs
@@ -122,10 +128,10 @@ template <typename T, int N> struct ZRCfg {
     static constexpr int SCR = SHFL ? PL : E * S;       // scratch line per warp (transposes, physical line)
     static_assert(SCR >= PL, "scratch holds a padded line");
     // index into the length-N table exp(-2 pi i j / N) of twiddle-table entry i
-    __host__ __device__ static constexpr int tw_index(int i) {
+    __host__ __device__ static constexpr int tw_index(int i, bool full = false) {
         const int row = i >> 5, l = i & 31;
         return SHFL ? (row < E - 1 ? (l * (row + 1)) % N : (E * l) % N)
-                    : (TWFULL ? (l * (row + 1)) % N : (l << row) % N);
+                    : ((full && TWFULL) ? (l * (row + 1)) % N : (l << row) % N);
     }
     // twiddle powers, scratch lines (one per warp; they also hold the physical
     // lines and the products), raw staging, mbarrier (16 B), kz table (ncp T)
@@ -237,8 +243,8 @@ __device__ __forceinline__ void zs_fft(int lane, V2<T> *x, const V2<T> *tws) {
 // lane + 32 m; on return x[q] is element k1 + E q + E^2 zr_sigma(j) of the
 // transform, with k1 = lane / G, j = lane % G.  The one transpose goes
 // through scr at offsets at(k1, i) (row k1 = 0..E-1, entry i = 0..31);
-// tws: the twiddle table of ZRCfg (rows tw_index).
-template <typename T, int N, int SIGN, class AT = ZrScratch<T, N>>
+// tws: the twiddle table of ZRCfg (rows tw_index(., FULLTW)).
+template <typename T, int N, int SIGN, class AT = ZrScratch<T, N>, bool FULLTW = false>
 __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<T> *tws, AT at = AT{}) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
@@ -251,7 +257,7 @@ __device__ __forceinline__ void zr_fft(int lane, V2<T> *x, V2<T> *scr, const V2<
     } else {
     Dft<E, SIGN, V>::run(x);
     {
-        if constexpr (Z::TWFULL) {   // every W^(lane k1) from the table
+        if constexpr (Z::TWFULL && FULLTW) {   // every W^(lane k1) from the table
 #pragma unroll
             for (int k1 = 1; k1 < E; ++k1) {
                 V t = tws[32 * (k1 - 1) + lane];
