@@ -151,7 +151,9 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             if (mul == V_IK_ROW) {
 #pragma unroll
                 for (int m = 0; m < E; ++m) {
-                    const T kr = (T)wavenum(lane + 32 * m, sp.n_row, sp.dk_row);
+                    const int ir = lane + 32 * m;   // row index; its wavenumber (Nyquist negative)
+                    const T kr = sizeof(T) == 8 ? (T)wavenum(ir, sp.n_row, sp.dk_row)
+                                                : (T)sp.dk_row * (T)(ir < sp.n_row / 2 ? ir : ir - sp.n_row);
                     x[m] = V{-kr * x[m].y, kr * x[m].x};
                 }
             } else if (mul == V_IK_OUT || mul == V_IK_COL) {
