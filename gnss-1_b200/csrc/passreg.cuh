@@ -89,7 +89,13 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
         o = sp.outer.expand(oc);
         c0 = (t % sp.ncolblk) * NB;
     };
-    // copy of one tile: thread -> column tid % NB, rows tid / NB + 32 k (kept rows only)
+    // copy of one tile: thread -> column tid % NB, rows tid / NB + 32 k (kept rows only).  The rows a thread
+    // copies, their source offsets within a tile (32-bit: a tile spans < 2^31 elements) and which are kept are
+    // the same for every tile of the launch.
+    static_assert(N / RSTEP <= 32, "one kept-row bit per copy sweep");
+    unsigned prow = 0;   // bit k: row tid / NB + RSTEP k is kept
+    for (int k = 0; k < N / RSTEP; ++k) prow |= (sp.row_in.kept(tid / NB + RSTEP * k) ? 1u : 0u) << k;
+    const int s_row = (int)sp.s_row;
     auto prefetch = [&](long long it, V *dst) {
         int fi, oc, o, c0;
         decode(it, fi, oc, o, c0);
@@ -97,10 +103,11 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
         const int b = tid % NB;
         if (c0 + b >= sp.ncols) return;
 #pragma unroll 4
-        for (int row = tid / NB; row < N; row += RSTEP) {
-            if (!sp.row_in.kept(row)) continue;
+        for (int k = 0; k < N / RSTEP; ++k) {
+            if (!((prow >> k) & 1u)) continue;
+            const int row = tid / NB + RSTEP * k;
             const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
-            const V *p = src + (long long)r * sp.s_row + b;
+            const V *p = src + r * s_row + b;
             if constexpr (sizeof(T) == 8) cp_async16(dst + row * LD + b, p, 16);
             else cp_async8(dst + row * LD + b, p, 8);
         }
