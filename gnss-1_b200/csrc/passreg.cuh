@@ -82,12 +82,15 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     long long item = blockIdx.x;
     if (item >= nitems) return;
     for (int i = tid; i < C::TWR * 32; i += NT) tws[i] = tw[Z::tw_index(i, true)];
+    // work items fit in 32 bits (inputs x outer indices x column blocks), so they are decoded with 32-bit
+    // divisions
     auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
-        fi = (int)(it / ntiles);
-        const int t = (int)(it % ntiles);
+        const int i32 = (int)it;
+        fi = i32 / ntiles;
+        const int t = i32 - fi * ntiles;
         oc = t / sp.ncolblk;
         o = sp.outer.expand(oc);
-        c0 = (t % sp.ncolblk) * NB;
+        c0 = (t - oc * sp.ncolblk) * NB;
     };
     // copy of one tile: thread -> column tid % NB, rows tid / NB + 32 k (kept rows only).  The rows a thread
     // copies, their source offsets within a tile (32-bit: a tile spans < 2^31 elements) and which are kept are
