@@ -794,13 +794,16 @@ __global__ void __launch_bounds__(STAT_SUMS * 32) k_stats_final(const double *__
 
 // ------------------------------------------------------------ reference-surface ops
 // Spectral index helpers for the transposed layout idx = kz + nz2*(x + nx*y).
+// A spectral field holds nx ny nz2 <= 512 * 512 * 257 < 2^32 modes, so the
+// index is split with 32-bit divisions.
 struct SpecIdx {
     int kx, ky, kz;
     __device__ __forceinline__ SpecIdx(long long idx, const Geom &g) {
-        kz = (int)(idx % g.nz2);
-        long long t = idx / g.nz2;
-        kx = (int)(t % g.nx);
-        ky = (int)(t / g.nx);
+        const unsigned i = (unsigned)idx, nz2 = (unsigned)g.nz2, nx = (unsigned)g.nx;
+        const unsigned t = i / nz2;
+        kz = (int)(i - t * nz2);
+        ky = (int)(t / nx);
+        kx = (int)(t - (unsigned)ky * nx);
     }
 };
 
