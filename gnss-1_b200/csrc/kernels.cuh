@@ -149,12 +149,14 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
     long long item = blockIdx.x;
     if (item >= nitems) return;
     // oc: compact outer index, o: expanded outer index
+    // work items fit in 32 bits (inputs x outer indices x column blocks): 32-bit divisions
     auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
-        fi = (int)(it / ntiles);
-        const int t = (int)(it % ntiles);
+        const int i32 = (int)it;
+        fi = i32 / ntiles;
+        const int t = i32 - fi * ntiles;
         oc = t / sp.ncolblk;
         o = sp.outer.expand(oc);
-        c0 = (t % sp.ncolblk) * NB;
+        c0 = (t - oc * sp.ncolblk) * NB;
     };
     auto prefetch = [&](long long it, V *dst) {
         int fi, oc, o, c0;
@@ -545,6 +547,19 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
     }
 }
 
+// A spectral field holds nx ny nz2 <= 512 * 512 * 257 < 2^32 modes, so the
+// index is split with 32-bit divisions.
+struct SpecIdx {
+    int kx, ky, kz;
+    __device__ __forceinline__ SpecIdx(long long idx, const Geom &g) {
+        const unsigned i = (unsigned)idx, nz2 = (unsigned)g.nz2, nx = (unsigned)g.nx;
+        const unsigned t = i / nz2;
+        kz = (int)(i - t * nz2);
+        ky = (int)(t / nx);
+        kx = (int)(t - (unsigned)ky * nx);
+    }
+};
+
 // statistics reductions (k_update with STATS, k_stats_partial, k_stats_final)
 constexpr int STAT_SUMS = 6;
 constexpr int STAT_BLOCKS = 1184;   // 8 x 148 SMs
@@ -745,9 +760,8 @@ k_stats_partial(FieldSet<T> st, int has_s, int has_c, Geom g, double *__restrict
     const long long nspec = (long long)g.nx * g.ny * g.nz2;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < nspec;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int kzi = (int)(idx % g.nz2);
-        const long long t = idx / g.nz2;
-        const int kxi = (int)(t % g.nx), kyi = (int)(t / g.nx);
+        const SpecIdx si(idx, g);
+        const int kzi = si.kz, kxi = si.kx, kyi = si.ky;
         const double k1 = wavenum(kxi, g.nx, g.dkx), k2 = wavenum(kyi, g.ny, g.dky), k3 = wavenum(kzi, g.nz, g.dkz);
         const double ksq = ksq3(k1, k2, k3);
         const double wt = (kzi == 0 || 2 * kzi == g.nz) ? 1.0 : 2.0;   // kz mirror (statistics.cu:1505-1532)
@@ -794,19 +808,6 @@ __global__ void __launch_bounds__(STAT_SUMS * 32) k_stats_final(const double *__
 
 // ------------------------------------------------------------ reference-surface ops
 // Spectral index helpers for the transposed layout idx = kz + nz2*(x + nx*y).
-// A spectral field holds nx ny nz2 <= 512 * 512 * 257 < 2^32 modes, so the
-// index is split with 32-bit divisions.
-struct SpecIdx {
-    int kx, ky, kz;
-    __device__ __forceinline__ SpecIdx(long long idx, const Geom &g) {
-        const unsigned i = (unsigned)idx, nz2 = (unsigned)g.nz2, nx = (unsigned)g.nx;
-        const unsigned t = i / nz2;
-        kz = (int)(i - t * nz2);
-        ky = (int)(t / nx);
-        kx = (int)(t - (unsigned)ky * nx);
-    }
-};
-
 #define GNSS_GRID_STRIDE(n) \
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (n); idx += (long long)gridDim.x * blockDim.x)
 
@@ -916,14 +917,16 @@ template <typename T> __global__ void k_shift_history(V2<T> *r, V2<T> *ro, long 
 }
 
 // physical-space point loop over x < nx, y < ny, z < nz of the padded layout
+// (nx ny nz <= 512^3 < 2^32 points: 32-bit divisions)
 struct PhysIdx {
     long long p;
     __device__ __forceinline__ PhysIdx(long long idx, const Geom &g) {
-        const int z = (int)(idx % g.nz);
-        const long long t = idx / g.nz;
-        const int y = (int)(t % g.ny);
-        const int x = (int)(t / g.ny);
-        p = (long long)z + 2LL * g.nz2 * ((long long)y + (long long)g.ny * x);
+        const unsigned i = (unsigned)idx, nz = (unsigned)g.nz, ny = (unsigned)g.ny;
+        const unsigned t = i / nz;
+        const int z = (int)(i - t * nz);
+        const unsigned x = t / ny;
+        const int y = (int)(t - x * ny);
+        p = (long long)z + 2LL * g.nz2 * ((long long)y + (long long)g.ny * (long long)x);
     }
 };
 
