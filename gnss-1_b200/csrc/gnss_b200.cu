@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -196,9 +197,12 @@ template <typename T, int N> struct Launch {
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;
                 cudaError_t e = prep_smem(kern, C::SMEM);
                 if (e != cudaSuccess) return e;
-                static int per_sm[2] = {0, 0};
-                int &ps = per_sm[sign < 0 ? 0 : 1];
-                if (ps == 0) ps = blocks_per_sm(kern, C::NT, C::SMEM);
+                static std::atomic<int> per_sm[2];   // resident blocks per SM, looked up once (any thread)
+                int ps = per_sm[sign < 0 ? 0 : 1].load(std::memory_order_relaxed);
+                if (ps == 0) {
+                    ps = blocks_per_sm(kern, C::NT, C::SMEM);
+                    per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
+                }
                 const long long nitems = (long long)sp.nin * sp.outer.count() * sp.ncolblk;
                 long long grid = (long long)ps * nsm;
                 if (grid > nitems) grid = nitems;
@@ -210,9 +214,12 @@ template <typename T, int N> struct Launch {
         auto kern = sign < 0 ? k_pass<T, N, -1> : k_pass<T, N, +1>;
         cudaError_t e = prep_smem(kern, C::SMEM);
         if (e != cudaSuccess) return e;
-        static int per_sm[2] = {0, 0};
-        int &ps = per_sm[sign < 0 ? 0 : 1];
-        if (ps == 0) ps = blocks_per_sm(kern, C::NT, C::SMEM);
+        static std::atomic<int> per_sm[2];   // resident blocks per SM, looked up once (any thread)
+        int ps = per_sm[sign < 0 ? 0 : 1].load(std::memory_order_relaxed);
+        if (ps == 0) {
+            ps = blocks_per_sm(kern, C::NT, C::SMEM);
+            per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
+        }
         const long long nitems = (long long)sp.nin * sp.outer.count() * sp.ncolblk;
         long long grid = (long long)ps * nsm;
         if (grid > nitems) grid = nitems;
