@@ -2,16 +2,25 @@
 """Throughput of the pseudospectral temporal-jet step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 512] [--precision mixed|fp64] [--scheme cnab2|rk3if]
+                    [--n 512] [--precision fp64|mixed] [--scalars 2] [--scheme cnab2|rk3if]
 
-Workload (default): one 512^3 periodic temporal jet, U(y) = 0.5(1+tanh((0.5-|y-pi|)/0.1)),
-one scalar with the same profile, seeded solenoidal noise of rms 0.05 on |k| <= 8,
-Re 5000, Sc 0.7, dt 2.5e-4, 2/3 dealiasing, the reference's Euler/AB2 + Crank-Nicolson
-scheme; state resident on the device.  A step is one full time step (nonlinear term,
-projection, dealiasing, update).  Metric: Mpoint-steps/s = N^3 * steps / s / 1e6,
-summed over GPUs (each GPU advances its own jet: replicas, no collective).
+Headline workload (default): one 512^3 periodic temporal jet in FP64 carrying the
+reference's field set u, v, w, s, c (the reference's solver_ps always advances both
+scalars; here c is a second passive scalar, alpha 0), Re 5000, Sc = Sc_c = 0.7,
+dt 2.5e-4, 2/3 dealiasing, the reference's Euler/AB2 + Crank-Nicolson scheme; state
+resident on the device.  A step is one full time step (nonlinear term, projection,
+dealiasing, update).  Metric: Mpoint-steps/s = N^3 * steps / s / 1e6, summed over
+GPUs (each GPU advances its own jet: replicas, no collective).  The same field set,
+grid, precision and scheme run in the reference arm, so the two values compare like
+for like.
 
-Rank 0 prints one JSON line.  Inputs (>= 1 GB per field) exceed L2 (126 MB), so no
+Legs beside the headline (each can be switched off): the mixed-precision form
+(FP32 transforms and storage, FP64 update coefficients and statistics) with one
+scalar at 512^3 against the FP64 step of the same field set, and its error against
+FP64 after 100 steps; the IF-RK3 scheme; the batched ensemble; the served stream
+(three runs); the reference program relinked against this library (drop-in shim).
+
+Rank 0 prints one JSON line.  Inputs (>= 0.5 GB per field) exceed L2 (126 MB), so no
 flush is needed between steps.  --impl reference runs the reference's own CUDA step
 (oracle/_ref/c512/refdrv built from the unmodified sources) on the same grid.
 """
@@ -33,9 +42,9 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "gnss-1_b200"))
 
-METRIC = "Mpoint-steps/s at 512^3 (mixed precision; FP64 alongside)"
+METRIC = "Mpoint-steps/s at 512^3, FP64, fields u v w s c (the reference's field set); mixed precision alongside"
 UNIT = "Mpoint-steps/s"
-RE, SC, DT, NOISE_K, AMP = 5000.0, 0.7, 2.5e-4, 8.0, 0.05
+RE, SC, SC_C, DT, NOISE_K, AMP = 5000.0, 0.7, 0.7, 2.5e-4, 8.0, 0.05
 E2E_STEPS_PER_CALL = 20
 
 
@@ -146,13 +155,14 @@ VARIANTS = {"auto": 0, "register": 1, "staged": 2, "warpspec": 3}
 ZNAMES = tuple(VARIANTS)   # variant names by value
 
 
-def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None, variants=None):
+def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4, barrier=None, variants=None,
+            n_scalars=1):
     """Time `steps` steps of one jet resident on `dev`; returns a dict."""
     cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
     nx, ny, nz = (n, n, n) if isinstance(n, int) else n
-    init = G.jet_initial_state(nx, ny, nz, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
-    ctx = G.Context(nx=nx, ny=ny, nz=nz, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme,
-                    device=dev)
+    init = G.jet_initial_state(nx, ny, nz, n_scalars=n_scalars, seed=0, noise_kmax=NOISE_K, amp=AMP)
+    ctx = G.Context(nx=nx, ny=ny, nz=nz, re=RE, sc=SC, sc_c=SC_C, dt=DT, n_scalars=n_scalars, precision=precision,
+                    scheme=scheme, device=dev)
     if variants:
         ctx.set_option(G.GNSS_OPT_ZVARIANT, VARIANTS[variants[0]])
         ctx.set_option(G.GNSS_OPT_PVARIANT, VARIANTS[variants[1]])
@@ -180,6 +190,7 @@ def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4,
         barrier()
     launches = ctx.launch_count() - l0
     ms = e0.elapsed_time(e1) / steps
+    ctx.check()
     stats = ctx.stats(st)
     # per-stage device times (separate profiled steps of the same workload)
     ctx.profile(True)
@@ -195,11 +206,21 @@ def run_leg(G, torch, n, precision, scheme, steps, warmup, dev, profile_steps=4,
     return out
 
 
-def run_e2e(G, torch, n, precision, scheme, calls, dev):
+def stage_table(leg) -> dict:
+    """Per-stage device ms per launch and algorithmic GB/s of a leg's profiled steps."""
+    prof = leg["profile"]
+    return {"stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()},
+            "stages_gbs": {k: round(leg["stage_bytes"][k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
+                           for k, v in prof.items() if v[1]}}
+
+
+def run_e2e(G, torch, n, precision, scheme, calls, dev, n_scalars=1):
     """Public host-buffer API: pinned state in, E2E_STEPS_PER_CALL steps, state and statistics out."""
     cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
-    init = [a.astype(cdt) for a in G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)]
-    ctx = G.Context(n, re=RE, sc=SC, dt=DT, n_scalars=1, precision=precision, scheme=scheme, device=dev)
+    init = [a.astype(cdt) for a in G.jet_initial_state(n, n_scalars=n_scalars, seed=0, noise_kmax=NOISE_K,
+                                                       amp=AMP)]
+    ctx = G.Context(n, re=RE, sc=SC, sc_c=SC_C, dt=DT, n_scalars=n_scalars, precision=precision, scheme=scheme,
+                    device=dev)
     host_in = torch.from_numpy(G.pack_state(init)).pin_memory()
     del init
     host_out = torch.empty_like(host_in).pin_memory()
@@ -240,10 +261,51 @@ def run_error_vs_fp64(G, torch, n, steps, dev) -> dict:
             del hi
     ref, got = res[G.GNSS_FP64], res[G.GNSS_FP32]
     errs = [float((g.to(torch.complex128) - r).norm() / r.norm()) for g, r in zip(got, ref)]
+    # the mean profiles (kx = kz = 0 line of u and s, statistics.cu:1936-2003)
+    prof = [float((got[q][:, 0, 0].to(torch.complex128) - ref[q][:, 0, 0]).norm() / ref[q][:, 0, 0].norm())
+            for q in (0, 3)]
     del res, ref, got
     torch.cuda.empty_cache()
     return {"steps": steps, "rel_l2_per_field": dict(zip(("u", "v", "w", "s"), [float(f"{e:.3e}") for e in errs])),
+            "mean_profile_rel_l2": {"u": float(f"{prof[0]:.3e}"), "s": float(f"{prof[1]:.3e}")},
             "max": float(f"{max(errs):.3e}"), "tolerance": 1e-5}
+
+
+def run_rk3(G, torch, n, precision, steps, dev) -> dict:
+    """The IF-RK3 scheme (three nonlinear evaluations per step) at n^3, one scalar."""
+    leg = run_leg(G, torch, n, precision, G.GNSS_SCHEME_RK3IF, steps, 3, dev, profile_steps=2)
+    pts = float(n) ** 3
+    step_bytes = 3.0 * sum(leg["stage_bytes"].values())
+    ms = leg["ms"]
+    peaks = measured_peaks()
+    out = {"value": round(pts / (ms * 1e-3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(ms, 4),
+           "steps": steps, "precision": "fp32" if precision == G.GNSS_FP32 else "fp64",
+           "launches_per_step": leg["launches"] / steps,
+           "workload": f"temporal jet {n}^3, 1 scalar, Re {RE:g}, Sc {SC}, dt {DT:g}, rk3if (3 substeps)",
+           "bytes_per_point_step": round(step_bytes / pts, 1),
+           "step_gbs": round(step_bytes / (ms * 1e-3) / 1e9, 1),
+           "step_frac_of_measured_hbm": round(step_bytes / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
+           "clocks": leg["clocks"]}
+    out.update(stage_table(leg))
+    return out
+
+
+def run_dropin(n, steps, warmup) -> dict | None:
+    """The reference's own driver relinked against this library through the
+    reference-ABI shim (oracle/_ref/c<n>/refdrv_gnss): the speed a user of the
+    reference's functions gets without changing their code."""
+    exe = ROOT / "oracle" / "_ref" / f"c{n}" / "refdrv_gnss"
+    if not exe.exists():
+        return None
+    r = subprocess.run([str(exe), "time", str(steps), str(warmup)], capture_output=True, text=True, timeout=1200)
+    if r.returncode != 0:
+        return {"error": r.stderr.strip()[-300:]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    ms = float(d["ms_per_step"])
+    return {"value": round(float(n) ** 3 / (ms * 1e-3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(ms, 4),
+            "steps": steps, "warmup": warmup,
+            "program": "reference driver + reference initialize/statistics/iofuncs objects, solver.o and "
+                       "fftfuncs.o replaced by refabi.cu over libgnss_b200.so; FP64, fields u v w s c"}
 
 
 # the batched ensemble workload: 16 x 64^3, 8 x 96^3, 6 x 128^3, 2 x 192^3
@@ -356,6 +418,17 @@ def run_serving(G, dev, duration_s=15.0, rate=4.0) -> dict:
                         "after an untimed warm-up request per (size, scalars)"}
 
 
+def run_serving_repeated(G, dev, runs=3, duration_s=15.0) -> dict:
+    """The served stream `runs` times (same seeded arrivals); the median run and the spread."""
+    outs = [run_serving(G, dev, duration_s) for _ in range(runs)]
+    order = sorted(range(runs), key=lambda i: outs[i]["p50_s"])
+    med = dict(outs[order[runs // 2]])
+    med["runs"] = [{k: o[k] for k in ("p50_s", "p99_s", "value", "completed", "failed")} for o in outs]
+    med["spread"] = {k: [min(o[k] for o in outs), max(o[k] for o in outs)] for k in ("p50_s", "p99_s", "value")}
+    med["reported"] = f"median run of {runs} by p50"
+    return med
+
+
 def cpu_baseline(n_sample=256, steps=2) -> dict:
     """The CPU oracle (same scheme and parameters) on all host cores, bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -363,9 +436,8 @@ def cpu_baseline(n_sample=256, steps=2) -> dict:
     import gnss_b200 as G
     O.build()
     cores = os.cpu_count() or 1
-    oc = O.cfg(n_sample, re=RE, sc=SC, dt=DT, nthreads=cores)
-    f = G.jet_initial_state(n_sample, n_scalars=1, seed=0, noise_kmax=NOISE_K, amp=AMP)
-    f.append(np.zeros_like(f[0]))
+    oc = O.cfg(n_sample, re=RE, sc=SC, sc_c=SC_C, dt=DT, nthreads=cores)
+    f = G.jet_initial_state(n_sample, n_scalars=2, seed=0, noise_kmax=NOISE_K, amp=AMP)
     r = [np.zeros_like(f[0]) for _ in range(5)]
     t0 = time.perf_counter()
     for s in range(steps):
@@ -373,8 +445,22 @@ def cpu_baseline(n_sample=256, steps=2) -> dict:
     dt = time.perf_counter() - t0
     return {"value": round(n_sample ** 3 * steps / dt / 1e6, 3), "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{steps} FP64 steps of the reference scheme (29 transforms/step, the reference's own "
-                      f"sequence, solver.cu:700-765) at {n_sample}^3 with the same parameters, "
-                      f"{dt:.1f} s on {cores} threads"}
+                      f"sequence, solver.cu:700-765) at {n_sample}^3 with the same parameters and fields "
+                      f"u v w s c, {dt:.1f} s on {cores} threads"}
+
+
+def headline_config(args, ws: int) -> dict:
+    """The `config` object of the headline line; both arms print the same one."""
+    prec = "fp64" if args.precision == "fp64" else "mixed"
+    shape = args.grid or f"{args.n}^3"
+    fields = "u v w s" + (" c" if args.scalars > 1 else "")
+    return {"workload": f"temporal jet {shape}, {prec}, fields {fields}"
+                        f"{' (c a second passive scalar, alpha 0)' if args.scalars > 1 else ''}, "
+                        f"Re {RE:g}, Sc {SC}{f', Sc_c {SC_C}' if args.scalars > 1 else ''}, dt {DT:g}, "
+                        f"2/3 dealias, {args.scheme}",
+            "grid": args.grid or args.n, "precision": prec, "scheme": args.scheme, "scalars": args.scalars,
+            "parallelism": f"replicas x{ws}",
+            "l2": "inputs larger than L2 (>= 0.5 GB per field); no flush"}
 
 
 def ours(args):
@@ -397,21 +483,15 @@ def ours(args):
     n = args.n
     shape = tuple(int(v) for v in args.grid.split("x")) if args.grid else (n, n, n)
     var = (args.z_variant, args.pass_variant)
-    leg = run_leg(G, torch, shape, prec, scheme, args.steps, args.warmup, dev, barrier=barrier, variants=var)
+    full = not args.grid
+    leg = run_leg(G, torch, shape, prec, scheme, args.steps, args.warmup, dev, barrier=barrier, variants=var,
+                  n_scalars=args.scalars)
     ms = leg["ms"] if red is None else red(leg["ms"])
     pts = float(shape[0] * shape[1] * shape[2])
     value = replica_value(pts, ms, ws)
-    fp64 = None
-    if prec == G.GNSS_FP32 and not args.no_fp64_leg:
-        l64 = run_leg(G, torch, shape, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 2, dev, barrier=barrier,
-                      variants=var)
-        ms64 = l64["ms"] if red is None else red(l64["ms"])
-        fp64 = {"value": round(replica_value(pts, ms64, ws), 3), "ms_per_step": round(ms64, 4),
-                "mixed_over_fp64": round(ms64 / ms, 3),
-                "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in l64["profile"].items()}}
     e2e = None
-    if not args.no_e2e and not args.grid:
-        e = run_e2e(G, torch, n, prec, scheme, args.e2e_calls, dev)
+    if not args.no_e2e and full:
+        e = run_e2e(G, torch, n, prec, scheme, args.e2e_calls, dev, n_scalars=args.scalars)
         ms_call = e["ms_call"] if red is None else red(e["ms_call"])
         e2e = {"value": round(replica_value(pts * E2E_STEPS_PER_CALL, ms_call, ws), 3), "unit": UNIT,
                "h2d_bytes_per_step": int(e["h2d"]), "d2h_bytes_per_step": int(e["d2h"]),
@@ -429,30 +509,52 @@ def ours(args):
     traffic_meas = None
     if tr_file.exists():
         tj = json.loads(tr_file.read_text())
-        key = f"{args.precision}:{args.grid or n}:{dom}"
+        key = f"{args.precision}:{args.scalars}:{args.grid or n}:{dom}"
         if key in tj:
             traffic_meas = tj[key]["bytes_per_launch"]
     roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic_meas,
-                "algorithmic_bytes": int(alg), "peak_source": peaks["source"] + " (burst copy)",
-                "stages_ms_per_launch": {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()},
-                "stages_gbs": {k: round(leg["stage_bytes"][k] / (v[0] / max(v[1], 1) * 1e-3) / 1e9, 1)
-                               for k, v in prof.items()}}
-    err = None
-    if prec == G.GNSS_FP32 and not args.no_error_check and not args.grid:
-        err = run_error_vs_fp64(G, torch, n, args.error_steps, dev)
+                "algorithmic_bytes": int(alg), "peak_source": peaks["source"] + " (burst copy)"}
+    roofline.update(stage_table(leg))
+    # the mixed-precision form (one scalar, FP32 transforms) against the FP64 step of the same field set
+    mixed = None
+    if prec == G.GNSS_FP64 and not args.no_mixed_leg:
+        l32 = run_leg(G, torch, shape, G.GNSS_FP32, scheme, max(args.steps, 10), 3, dev, barrier=barrier,
+                      variants=var, n_scalars=1)
+        l64 = run_leg(G, torch, shape, G.GNSS_FP64, scheme, max(3, min(args.steps, 10)), 3, dev, barrier=barrier,
+                      variants=var, n_scalars=1)
+        ms32 = l32["ms"] if red is None else red(l32["ms"])
+        ms64 = l64["ms"] if red is None else red(l64["ms"])
+        mixed = {"value": round(replica_value(pts, ms32, ws), 3), "unit": UNIT, "ms_per_step": round(ms32, 4),
+                 "dtype": "f32", "fields": "u v w s",
+                 "fp64_same_fields": {"value": round(replica_value(pts, ms64, ws), 3), "ms_per_step": round(ms64, 4)},
+                 "mixed_over_fp64": round(ms64 / ms32, 3), "clocks": l32["clocks"]}
+        mixed.update(stage_table(l32))
+        mixed["fp64_same_fields"].update(stage_table(l64))
+        dom32 = max(l32["profile"], key=lambda k: l32["profile"][k][0])
+        t32, n32 = l32["profile"][dom32]
+        a32 = l32["stage_bytes"][dom32] / (t32 / n32 * 1e-3) / 1e9
+        mixed["roofline"] = {"kernel": dom32, "achieved": round(a32, 1), "frac": round(a32 / peaks["hbm_gbs"], 4)}
+        if full and not args.no_error_check:
+            mixed["error_vs_fp64"] = run_error_vs_fp64(G, torch, n, args.error_steps, dev)
+    rk3 = None
+    if full and not args.no_rk3:
+        rk3 = run_rk3(G, torch, n, G.GNSS_FP32, args.rk3_steps, dev)
     ens = None
-    if not args.no_ensemble and not args.grid:
+    if not args.no_ensemble and full:
         ens = run_ensemble(G, torch, dev, args.ensemble_steps, args.ensemble_branches)
         if red is not None:
             ens["value"] = round(ws * ens["points_per_step"] / (red(ens["ms_per_step"]) * 1e-3) / 1e6, 3)
     serve = None
-    if not args.no_serve and not args.grid:
-        serve = run_serving(G, dev, args.serve_seconds)
+    if not args.no_serve and full:
+        serve = run_serving_repeated(G, dev, args.serve_runs, args.serve_seconds)
         if red is not None:   # whole-job throughput: every rank served its own stream
             serve["value"] = round(sum_over_ranks(serve["value"]), 3)
             serve["p50_s"] = red(serve["p50_s"])
             serve["p99_s"] = red(serve["p99_s"])
+    dropin = None
+    if rank == 0 and ws == 1 and full and not args.no_dropin:
+        dropin = run_dropin(n, max(3, min(args.steps, 10)), 2)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -466,15 +568,11 @@ def ours(args):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if prec == G.GNSS_FP32 else "f64", "data": "synthetic",
-        "config": {"workload": f"temporal jet {'x'.join(map(str, shape)) if args.grid else f'{n}^3'}, "
-                               f"1 scalar, Re {RE:g}, Sc {SC}, dt {DT:g}, "
-                               f"noise |k|<={NOISE_K:g} rms {AMP}, 2/3 dealias, {args.scheme}",
-                   "grid": n, "precision": args.precision, "scheme": args.scheme,
-                   "kernels": {"z": args.z_variant, "pass": args.pass_variant},
-                   "parallelism": f"replicas x{ws}",
-                   "l2": "inputs larger than L2 (>= 0.5 GB per field); no flush"},
+        "config": headline_config(args, ws),
+        "initial_state": f"seeded solenoidal noise |k|<={NOISE_K:g} rms {AMP} on the tanh jet profiles",
+        "kernels": {"z": args.z_variant, "pass": args.pass_variant},
         "gpu_launches": leg["launches"], "clocks": leg["clocks"], "e2e": e2e, "roofline": roofline,
-        "cpu_baseline": cpu, "fp64": fp64, "error_vs_fp64": err, "ensemble": ens, "serving": serve,
+        "cpu_baseline": cpu, "mixed": mixed, "rk3if": rk3, "ensemble": ens, "serving": serve, "dropin": dropin,
         "stats_after": {k: leg["stats"][k] for k in ("ke", "eps", "chi_s", "var_s")},
     }
     print(json.dumps(line), flush=True)
@@ -503,9 +601,10 @@ def reference(args):
         "metric": METRIC, "impl": "reference", "value": round(value, 3), "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"temporal jet {args.n}^3, Re {RE:g}, Sc {SC}, dt {DT:g}, 2/3 dealias, cnab2 "
-                               f"(reference solver_ps; always carries both scalars s and c)",
-                   "grid": args.n, "precision": "fp64", "scheme": "cnab2", "parallelism": "single GPU"},
+        "config": headline_config(argparse.Namespace(**{**vars(args), "precision": "fp64", "scalars": 2}), 1),
+        "initial_state": "the reference's jet profiles (initializeVelocity / initializeScalar), no noise",
+        "program": "the reference's solver_ps (cuFFT; it always advances u v w s c) from the unmodified "
+                   "sources built -O3 for sm_100a",
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": "the reference's own CUDA step (cuFFT, sm_100a build of the unmodified "
@@ -524,11 +623,16 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--grid", default=None, help="NXxNYxNZ instead of n^3 (profiling workloads; no e2e leg)")
-    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--scalars", type=int, choices=(1, 2), default=2)
     ap.add_argument("--scheme", choices=("cnab2", "rk3if"), default="cnab2")
     ap.add_argument("--e2e-calls", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-fp64-leg", action="store_true")
+    ap.add_argument("--no-mixed-leg", action="store_true")
+    ap.add_argument("--no-rk3", action="store_true")
+    ap.add_argument("--rk3-steps", type=int, default=5)
+    ap.add_argument("--no-dropin", action="store_true")
+    ap.add_argument("--serve-runs", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--z-variant", choices=tuple(VARIANTS), default="auto")
     ap.add_argument("--pass-variant", choices=("auto", "register", "staged"), default="auto")

@@ -51,14 +51,30 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, unsigned parity) {
 }
 
 // Waits for the phase with the given parity to complete; gives up after
-// about 2^24 polls (a few seconds) and returns false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
-    for (unsigned i = 0; i < (1u << 24); ++i) {
+// `limit` polls (by default 2^24, a few seconds) and returns false.
+constexpr unsigned WAIT_POLLS = 1u << 24;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, unsigned limit = WAIT_POLLS) {
+    for (unsigned i = 0; i < limit; ++i) {
         if (mbar_test(bar, parity)) return true;
         if (i > 32) __nanosleep(128);
     }
     return false;
 }
+
+// Control of the bounded waits of a kernel, read from err[1] (err[0] is the
+// error word): 0 in normal operation.  A nonzero value v is a test of the
+// time-out path: every wait gives up after v polls, and block 0 arms its
+// first mbarrier phase without issuing the copies that would complete it,
+// so that wait runs out with no copy in flight.
+struct WaitCtl {
+    unsigned limit;
+    bool withhold;   // this block withholds the copies of its first phase
+    __device__ __forceinline__ explicit WaitCtl(const unsigned *err) {
+        const unsigned v = err[1];
+        limit = v ? v : WAIT_POLLS;
+        withhold = v != 0 && blockIdx.x == 0;
+    }
+};
 
 // Named barrier `id` (1..15; 0 is __syncthreads) over `nthreads` threads,
 // whole warps; true on every participant when pred is true on any of them.

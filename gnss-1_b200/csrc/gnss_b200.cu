@@ -59,7 +59,9 @@ struct gnss_ctx {
     ZRecipeSet zrec{};
     std::string err;
     long long launches = 0;                       // kernels launched by this context
-    unsigned *d_err = nullptr;                    // device error word set by bounded waits that time out
+    unsigned *d_err = nullptr;                    // [0] error word set by bounded waits that time out,
+                                                  // [1] wait control (GNSS_OPT_TEST_WAIT; 0 normally)
+    int test_wait = 0;                            // GNSS_OPT_TEST_WAIT
     int nsm = 148;                                // SMs of the device
     bool profiling = false;
     std::vector<cudaEvent_t> ev_pool;             // profiling events, reused
@@ -978,6 +980,14 @@ gnss_status gnss_stage_bytes(const gnss_ctx *c, double *bytes) {
 
 gnss_status gnss_set_option(gnss_ctx *c, int key, int value) {
     if (!c) return GNSS_ERR_INVALID;
+    if (key == GNSS_OPT_TEST_WAIT) {   // poll cap of the z kernel's waits; block 0 withholds its first copy
+        if (value < 0) return fail(c, GNSS_ERR_INVALID, "bad poll cap %d", value);
+        CK(c, cudaSetDevice(c->cfg.device));
+        const unsigned v = (unsigned)value;
+        CK(c, cudaMemcpy(c->d_err + 1, &v, sizeof v, cudaMemcpyHostToDevice));
+        c->test_wait = value;
+        return GNSS_OK;
+    }
     if (key != GNSS_OPT_ZVARIANT && key != GNSS_OPT_PVARIANT) return fail(c, GNSS_ERR_INVALID, "unknown option %d", key);
     const int top = key == GNSS_OPT_ZVARIANT ? GNSS_VARIANT_WARPSPEC : GNSS_VARIANT_STAGED;
     if (value < GNSS_VARIANT_AUTO || value > top)
@@ -996,6 +1006,7 @@ gnss_status gnss_get_option(const gnss_ctx *c, int key, int *value) {
     if (!c || !value) return GNSS_ERR_INVALID;
     if (key == GNSS_OPT_ZVARIANT) *value = c->zvariant;
     else if (key == GNSS_OPT_PVARIANT) *value = c->pvariant;
+    else if (key == GNSS_OPT_TEST_WAIT) *value = c->test_wait;
     else if (key == GNSS_OPT_ZKERNEL)
         *value = c->cfg.precision == GNSS_FP64 ? zkernel_of<double>(c) : zkernel_of<float>(c);
     else return GNSS_ERR_INVALID;
@@ -1243,7 +1254,8 @@ gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out) {
         return GNSS_ERR_NOMEM;
     }
     c->owned_bytes += sizeof(double) * (STAT_BLOCKS * STAT_SUMS + STAT_SUMS);
-    if (cudaMalloc(&c->d_err, sizeof(unsigned)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(unsigned)) != cudaSuccess) {
+    if (cudaMalloc(&c->d_err, 2 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(c->d_err, 0, 2 * sizeof(unsigned)) != cudaSuccess) {
         cudaGetLastError();
         gnss_destroy(c);
         return GNSS_ERR_NOMEM;
@@ -1740,16 +1752,25 @@ static gnss_status noalloc_pool_address(int dev, void **out) {
     return GNSS_OK;
 }
 
+// One twiddle table, passed by value in the launch's parameters (at most
+// GNSS_NOALLOC_TW complex values: 8 KB in FP64) and written to its slot of the
+// array by a small kernel, so no host buffer is copied and the values are the
+// same long-double ones as a context's tables.
+template <typename T> struct NoallocTable { V2<T> v[GNSS_NOALLOC_TW]; };
+template <typename T> __global__ void k_noalloc_table(V2<T> *dst, int n, const __grid_constant__ NoallocTable<T> t) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = t.v[k];
+}
+
 template <typename T> static cudaError_t noalloc_twiddles(V2<T> *dst, int n, cudaStream_t s) {
-    V2<T> h[GNSS_NOALLOC_TW];
+    NoallocTable<T> h;
     const long double twopi = 6.283185307179586476925286766559L;
     for (int k = 0; k < n; ++k) {
         long double a = twopi * (long double)k / (long double)n;
-        h[k].x = (T)cosl(a);
-        h[k].y = (T)(-sinl(a));
+        h.v[k].x = (T)cosl(a);
+        h.v[k].y = (T)(-sinl(a));
     }
-    // pageable source: the call returns once the table has been staged
-    return cudaMemcpyAsync(dst, h, sizeof(V2<T>) * n, cudaMemcpyHostToDevice, s);
+    k_noalloc_table<T><<<1, 256, 0, s>>>(dst, n, h);
+    return cudaGetLastError();
 }
 
 template <typename T> static gnss_status noalloc_forward_t(gnss_ctx *c, void *field, cudaStream_t s) {
@@ -1792,6 +1813,13 @@ gnss_status gnss_forward_noalloc(const gnss_config *cfg, void *field, void *stre
     c.tw[0] = pool;
     c.scratch = reinterpret_cast<double2 *>(pool) + 3 * GNSS_NOALLOC_TW;
     c.nscratch = 1;
-    cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, k.device);
-    return PREC_CALL(&c, noalloc_forward_t, &c, field, S(stream));
+    if (cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, k.device) != cudaSuccess) {
+        cudaGetLastError();
+        std::fprintf(stderr, "gnss_forward_noalloc: cannot read the SM count of device %d\n", k.device);
+        return GNSS_ERR_CUDA;
+    }
+    st = PREC_CALL(&c, noalloc_forward_t, &c, field, S(stream));
+    // there is no context to keep the message in: print it
+    if (st) std::fprintf(stderr, "gnss_forward_noalloc: %s\n", c.err.c_str());
+    return st;
 }

@@ -497,21 +497,23 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
         }
         __syncthreads();
     }
-    auto issue = [&](long long p) {
+    const WaitCtl wc(err);
+    auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
-        for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+        if (!withhold)
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
     };
-    if (pipe && threadIdx.x == 0) issue(pair);
+    if (pipe && threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
     V *lineA = bankA + warp * LEN;
     const ZRecipe rc = zr.q[warp];
     for (; pair < npairs; pair += gridDim.x) {
         const V *a0, *a1;
         if (pipe) {
-            const bool ok = mbar_wait_bounded(bar, parity);
+            const bool ok = mbar_wait_bounded(bar, parity, wc.limit);
             if (__syncthreads_or(!ok)) {
                 if (threadIdx.x == 0) atomicOr(err, 1u);
-                mbar_wait_bounded(bar, parity);   // let an overdue copy land before leaving
+                mbar_wait_bounded(bar, parity, wc.limit);   // let an overdue copy land before leaving
                 return;
             }
             parity ^= 1u;

@@ -556,20 +556,22 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
         mbar_fence_init();
     }
     __syncthreads();
-    auto issue = [&](long long p) {
+    const WaitCtl wc(err);
+    auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
-        for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+        if (!withhold)
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
     };
-    if (threadIdx.x == 0) issue(pair);
+    if (threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
     const ZRecipe rc = zr.q[warp];
     const int kind = zr_kind(rc);
     V *scr = scr_all + warp * SCR;   // transposes, then this warp's physical quantity
     for (; pair < npairs; pair += gridDim.x) {
-        const bool ok = mbar_wait_bounded(bar, parity);
+        const bool ok = mbar_wait_bounded(bar, parity, wc.limit);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(err, 1u);
-            mbar_wait_bounded(bar, parity);   // let an overdue copy land before leaving
+            mbar_wait_bounded(bar, parity, wc.limit);   // let an overdue copy land before leaving
             return;
         }
         parity ^= 1u;
@@ -664,11 +666,13 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
         mbar_fence_init();
     }
     __syncthreads();
-    auto issue = [&](long long p) {
+    const WaitCtl wc(err);
+    auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
-        for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+        if (!withhold)
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
     };
-    if (threadIdx.x == 0) issue(pair);
+    if (threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
     const bool inv = warp < NPH;
     const ZRecipe rc = zr.q[inv ? warp : 0];
@@ -677,14 +681,14 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
     for (;;) {
         if (inv) {
             if (pair < npairs) {
-                const bool ok = mbar_wait_bounded(bar, parity);
+                const bool ok = mbar_wait_bounded(bar, parity, wc.limit);
                 V x[E];
                 zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp,
                               keep, tkz);
                 if (bar_named_or(1, NINV, !ok)) {   // every inverse warp has unpacked, or one gave up
                     if (threadIdx.x == 0) {
                         stop = 1;
-                        mbar_wait_bounded(bar, parity);   // let an overdue copy land before leaving
+                        mbar_wait_bounded(bar, parity, wc.limit);   // let an overdue copy land before leaving
                     }
                 } else {
                     parity ^= 1u;

@@ -35,6 +35,8 @@ GNSS_NSTATS = 7
 GNSS_OPT_ZVARIANT = 0
 GNSS_OPT_PVARIANT = 1
 GNSS_OPT_ZKERNEL = 2   # read-only: the z kernel the options select
+GNSS_OPT_TEST_WAIT = 3  # test of the bounded device waits: poll cap, first copy of block 0 withheld (0 = off)
+GNSS_ERR_TIMEOUT = 5
 GNSS_VARIANT_AUTO = GNSS_ZVARIANT_AUTO = 0
 GNSS_VARIANT_REGISTER = GNSS_ZVARIANT_REGISTER = 1
 GNSS_VARIANT_STAGED = GNSS_ZVARIANT_STAGED = 2

@@ -258,6 +258,12 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 #define GNSS_OPT_PVARIANT 1
 #define GNSS_OPT_ZKERNEL 2   /* read-only (gnss_get_option): the z kernel the options select for this
                               * context, GNSS_VARIANT_WARPSPEC, _REGISTER or _STAGED */
+#define GNSS_OPT_TEST_WAIT 3 /* test of the bounded device waits, 0 (default) = off.  A value v > 0 caps
+                              * every wait of the fused z kernels at v polls, and the first block withholds
+                              * the copies of its first line pair (the mbarrier phase is armed, no copy is
+                              * issued), so its wait runs out with nothing in flight: the block stops, the
+                              * step's result is incomplete, and the next gnss_check (or gnss_stats,
+                              * gnss_run_host) returns GNSS_ERR_TIMEOUT.  For tests of that path only. */
 #define GNSS_VARIANT_AUTO 0
 #define GNSS_VARIANT_REGISTER 1
 #define GNSS_VARIANT_STAGED 2
@@ -433,7 +439,10 @@ gnss_status gnss_initial_jet(gnss_ctx *ctx, const gnss_jet_params *p, const gnss
  * before any stream capture.  All calls share the array and keep the last
  * call's contents in it; calls that overlap on the GPU (any stream, any
  * thread) race and must be serialised by the caller.  Only cfg's sizes, box
- * lengths, precision and device are used. */
+ * lengths, precision and device are used.  The twiddle tables reach the
+ * device as launch parameters of a small kernel, not through a host buffer.
+ * With no context to hold a message, a failure other than a rejected
+ * argument prints its reason to stderr. */
 #define GNSS_NOALLOC_MAX_ELEMS 1114112
 gnss_status gnss_forward_noalloc(const gnss_config *cfg, void *field, void *stream);
 

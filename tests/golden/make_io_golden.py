@@ -27,7 +27,7 @@ FILES = ["u.3", "vis/u_xy.3", "vis/u_xz.3", "vis/u_yz.3", "stats/KE", "Yprofs/u_
 def main() -> int:
     if not EXE.exists():
         subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh"), "g12"], check=True)
-    with tempfile.TemporaryDirectory(dir=ROOT / "_work" if (ROOT / "_work").exists() else None) as tmp:
+    with tempfile.TemporaryDirectory() as tmp:
         subprocess.run([str(EXE), "io"], cwd=tmp, check=True, stdout=subprocess.DEVNULL)
         if OUT.exists():
             shutil.rmtree(OUT)

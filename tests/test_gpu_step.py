@@ -189,3 +189,73 @@ def test_run_host_matches_device_steps(torch_cuda, shape, scheme, precision, ns,
         assert 0 < h2d < d2h
         ctx.run_host(host, host, steps, True, None)   # in place, no statistics
         assert np.array_equal(host.numpy(), out.numpy())
+
+
+@pytest.mark.gpu
+def test_mixed_precision_config3_128(torch_cuda):
+    """The mixed-precision form with the 512^3 jet's parameters (Re 5000, Sc 0.7,
+    dt 2.5e-4, one scalar, noise |k| <= 8 rms 0.05) at 128^3: every field within
+    1e-5 relative L2 of the FP64 step after 100 steps from the same state."""
+    import gnss_b200 as G
+    torch = torch_cuda
+    n, re, sc, dt, steps = 128, 5000.0, 0.7, 2.5e-4, 100
+    init = G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=8.0, amp=0.05)
+    out = {}
+    for prec, cdt in ((G.GNSS_FP64, np.complex128), (G.GNSS_FP32, np.complex64)):
+        with G.Context(n, re=re, sc=sc, dt=dt, n_scalars=1, precision=prec) as ctx:
+            st = [to_dev(torch, a.astype(cdt)) for a in init]
+            hi = [torch.zeros_like(st[0]) for _ in st]
+            ctx.de_alias(st)
+            for s in range(steps):
+                ctx.solver_ps(st, hi, euler=(s == 0))
+            ctx.check()
+            out[prec] = [to_host(t) for t in st]
+    for q, name in enumerate("uvws"):
+        err = rel_l2(out[G.GNSS_FP32][q].astype(np.complex128), out[G.GNSS_FP64][q])
+        assert err < 1e-5, f"{name}: rel L2 {err:.3e} after {steps} steps"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_bounded_wait_timeout_is_reported(torch_cuda, oracle, precision):
+    """A bounded device wait that runs out is reported, and nothing hangs.
+
+    GNSS_OPT_TEST_WAIT caps the z kernel's mbarrier waits at 1024 polls and
+    makes its first block arm the barrier of its first line pair without
+    issuing the copies (nothing is in flight), so that wait runs out: the
+    block sets the error word and returns, the launch completes, and
+    gnss_check reports GNSS_ERR_TIMEOUT once (the word is then cleared).  The
+    context stays usable, and a fresh context steps correctly afterwards.
+    """
+    import gnss_b200 as G
+    torch = torch_cuda
+    n, re, dt = 64, 1000.0, 1e-3
+    cdt = np.complex128 if precision == G.GNSS_FP64 else np.complex64
+    init = _initial(G, n, 1)
+    with G.Context(n, re=re, dt=dt, n_scalars=1, precision=precision) as ctx:
+        st = [to_dev(torch, a.astype(cdt)) for a in init]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        ctx.de_alias(st)
+        ctx.set_option(G.GNSS_OPT_TEST_WAIT, 1024)
+        assert ctx.get_option(G.GNSS_OPT_TEST_WAIT) == 1024
+        ctx.solver_ps(st, hi, euler=True)
+        with pytest.raises(G.GnssError) as ei:
+            ctx.check()
+        assert ei.value.status == G.GNSS_ERR_TIMEOUT
+        ctx.check()                       # reported once, then cleared
+        ctx.set_option(G.GNSS_OPT_TEST_WAIT, 0)
+        ctx.solver_ps(st, hi, euler=False)
+        ctx.check()
+    # a fresh context: one step against the oracle
+    oc = oracle.cfg(n, re=re, dt=dt)
+    ref = _oracle_run(oracle, oc, init, 1, 1)
+    with G.Context(n, re=re, dt=dt, n_scalars=1, precision=precision) as ctx:
+        st = [to_dev(torch, a.astype(cdt)) for a in init]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        ctx.de_alias(st)
+        ctx.solver_ps(st, hi, euler=True)
+        ctx.check()
+        tol = 1e-12 if precision == G.GNSS_FP64 else 1e-5
+        for q in range(4):
+            err = rel_l2(to_host(st[q]).astype(np.complex128), ref[0][0][q])
+            assert err < tol, f"field {q}: {err:.3e}"
