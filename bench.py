@@ -151,7 +151,7 @@ def measured_peaks() -> dict:
 
 
 # ------------------------------------------------------------------ our arm
-VARIANTS = {"auto": 0, "register": 1, "staged": 2, "warpspec": 3}
+VARIANTS = {"auto": 0, "register": 1, "staged": 2, "warpspec": 3, "tensor": 4}
 ZNAMES = tuple(VARIANTS)   # variant names by value
 
 
@@ -635,7 +635,7 @@ def main():
     ap.add_argument("--serve-runs", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--z-variant", choices=tuple(VARIANTS), default="auto")
-    ap.add_argument("--pass-variant", choices=("auto", "register", "staged"), default="auto")
+    ap.add_argument("--pass-variant", choices=("auto", "register", "staged", "tensor"), default="auto")
     ap.add_argument("--no-error-check", action="store_true")
     ap.add_argument("--error-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")

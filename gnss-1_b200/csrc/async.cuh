@@ -70,7 +70,7 @@ struct WaitCtl {
     unsigned limit;
     bool withhold;   // this block withholds the copies of its first phase
     __device__ __forceinline__ explicit WaitCtl(const unsigned *err) {
-        const unsigned v = err[1];
+        const unsigned v = err ? err[1] : 0u;
         limit = v ? v : WAIT_POLLS;
         withhold = v != 0 && blockIdx.x == 0;
     }

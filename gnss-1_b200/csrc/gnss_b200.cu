@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "zreg.cuh"
 #include "passreg.cuh"
+#include "passtc.cuh"
 #include "diag.cuh"
 
 using namespace gnss;
@@ -62,6 +63,8 @@ struct gnss_ctx {
     unsigned *d_err = nullptr;                    // [0] error word set by bounded waits that time out,
                                                   // [1] wait control (GNSS_OPT_TEST_WAIT; 0 normally)
     int test_wait = 0;                            // GNSS_OPT_TEST_WAIT
+    double2 *mean64 = nullptr;                    // FP32 contexts: FP64 mean-profile line (kx = kz = 0) of the
+                                                  // state and history, [2][5][ny] (k_update)
     int nsm = 148;                                // SMs of the device
     bool profiling = false;
     std::vector<cudaEvent_t> ev_pool;             // profiling events, reused
@@ -187,13 +190,38 @@ __host__ __device__ constexpr bool zr_auto_pass(int n, bool fp64) {
 
 template <typename T, int N> struct Launch {
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
-                            cudaStream_t s, int pvariant) {
+                            cudaStream_t s, int pvariant, unsigned *err) {
+        if constexpr (sizeof(T) == 4 && ptc_size(N)) {
+            // split-TF32 DFT-GEMM transforms on the tensor cores (tiles of 8 columns)
+            if (pvariant == GNSS_VARIANT_TENSOR) {
+                using C = PTCfg<N>;
+                auto kern = sign < 0 ? k_passtc<N, -1> : k_passtc<N, +1>;
+                cudaError_t e = prep_smem(kern, C::SMEM);
+                if (e != cudaSuccess) return e;
+                static std::atomic<int> per_sm[2];   // resident blocks per SM, looked up once (any thread)
+                int ps = per_sm[sign < 0 ? 0 : 1].load(std::memory_order_relaxed);
+                if (ps == 0) {
+                    ps = blocks_per_sm(kern, C::NT, C::SMEM);
+                    per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
+                }
+                PassSpec s8 = sp;
+                const int cols = sp.ncols > sp.out_ncols ? sp.ncols : sp.out_ncols;
+                s8.ncolblk = (cols + C::NB - 1) / C::NB;
+                const long long nitems = (long long)s8.nin * s8.outer.count() * s8.ncolblk;
+                long long grid = (long long)ps * nsm;
+                if (grid > nitems) grid = nitems;
+                kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(reinterpret_cast<const PassPtrs<float> &>(P), s8,
+                                                            reinterpret_cast<const float2 *>(tw), err);
+                return cudaGetLastError();
+            }
+        }
         if constexpr (zr_size(N)) {
             // register-resident column transforms where they measured faster (512^3 FP32 step 7.34 against
             // 8.39 ms, FP64 10.1 against 8.9 Gpoint-steps/s; 256^3 1.23 against 1.28 ms; N = 96 .. 192 with
             // lane shuffles)
             const bool reg = pvariant == GNSS_VARIANT_REGISTER ||
-                             (pvariant == GNSS_VARIANT_AUTO && zr_auto_pass(N, sizeof(T) == 8));
+                             ((pvariant == GNSS_VARIANT_AUTO || pvariant == GNSS_VARIANT_TENSOR) &&
+                              zr_auto_pass(N, sizeof(T) == 8));
             if (reg) {
                 using C = PRCfg<T, N>;
                 auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;
@@ -395,8 +423,8 @@ template <typename T, int N> struct Launch {
 
 template <typename T>
 static cudaError_t launch_pass(int n, int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
-                               cudaStream_t s, int pvariant) {
-    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::pass(sign, P, sp, tw, nsm, s, pvariant)));
+                               cudaStream_t s, int pvariant, unsigned *err) {
+    GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::pass(sign, P, sp, tw, nsm, s, pvariant, err)));
 }
 template <typename T>
 static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfields, long long nlines, int nz2, T scale,
@@ -581,10 +609,10 @@ template <typename T> static gnss_status forward_t(gnss_ctx *c, void *f, cudaStr
     PassPtrs<T> P{};
     P.in[0] = F.p[0];
     P.out[0] = X;
-    CK(c, launch_pass<T>(g.ny, -1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s, c->pvariant));
+    CK(c, launch_pass<T>(g.ny, -1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s, c->pvariant, c->d_err));
     P.in[0] = X;
     P.out[0] = F.p[0];
-    CK(c, launch_pass<T>(g.nx, -1, P, pass_spec<T>(c, X_FWD, 1), c->tw[0], c->nsm, s, c->pvariant));
+    CK(c, launch_pass<T>(g.nx, -1, P, pass_spec<T>(c, X_FWD, 1), c->tw[0], c->nsm, s, c->pvariant, c->d_err));
     return GNSS_OK;
 }
 
@@ -601,10 +629,10 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
     PassPtrs<T> P{};
     P.in[0] = F.p[0];
     P.out[0] = X;
-    CK(c, launch_pass<T>(g.nx, +1, P, pass_spec<T>(c, X_INV, 1), c->tw[0], c->nsm, s, c->pvariant));
+    CK(c, launch_pass<T>(g.nx, +1, P, pass_spec<T>(c, X_INV, 1), c->tw[0], c->nsm, s, c->pvariant, c->d_err));
     P.in[0] = X;
     P.out[0] = F.p[0];
-    CK(c, launch_pass<T>(g.ny, +1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s, c->pvariant));
+    CK(c, launch_pass<T>(g.ny, +1, P, pass_spec<T>(c, Y_PASS, 1), c->tw[1], c->nsm, s, c->pvariant, c->d_err));
     CK(c, launch_zpass<T>(g.nz, +1, F, 1, nlines, g.nz2, scale, c->tw[2], s));
     return GNSS_OK;
 }
@@ -654,7 +682,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             spx.nvar[i] = c->xvar_n[i];
             for (int v = 0; v < 2; ++v) { spx.vmul[i][v] = c->xvar_mul[i][v]; spx.vout[i][v] = c->xvar_out[i][v]; }
         }
-        CK(c, launch_pass<T>(g.nx, +1, P, spx, c->tw[0], c->nsm, s, c->pvariant));
+        CK(c, launch_pass<T>(g.nx, +1, P, spx, c->tw[0], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 1);
@@ -666,7 +694,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             spy.nvar[i] = c->yvar_n[i];
             for (int v = 0; v < 2; ++v) { spy.vmul[i][v] = c->yvar_mul[i][v]; spy.vout[i][v] = c->yvar_out[i][v]; }
         }
-        CK(c, launch_pass<T>(g.ny, +1, P, spy, c->tw[1], c->nsm, s, c->pvariant));
+        CK(c, launch_pass<T>(g.ny, +1, P, spy, c->tw[1], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 2);
@@ -677,13 +705,13 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
         StageTimer t(c, s, 3);
         PassPtrs<T> P{};
         for (int q = 0; q < nnl; ++q) { P.in[q] = Qf(q); P.out[q] = Pf(q); }
-        CK(c, launch_pass<T>(g.ny, -1, P, step_spec<T>(c, Y_FWD_STEP, nnl), c->tw[1], c->nsm, s, c->pvariant));
+        CK(c, launch_pass<T>(g.ny, -1, P, step_spec<T>(c, Y_FWD_STEP, nnl), c->tw[1], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 4);
         PassPtrs<T> P{};
         for (int q = 0; q < nnl; ++q) { P.in[q] = Pf(q); P.out[q] = R.p[q]; }
-        CK(c, launch_pass<T>(g.nx, -1, P, step_spec<T>(c, X_FWD_STEP, nnl), c->tw[0], c->nsm, s, c->pvariant));
+        CK(c, launch_pass<T>(g.nx, -1, P, step_spec<T>(c, X_FWD_STEP, nnl), c->tw[0], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 5);
@@ -695,10 +723,10 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             nblk = std::min<long long>(nblk, STAT_BLOCKS);
             if (uc.scheme == GNSS_SCHEME_CNAB2)
                 k_update<T, GNSS_SCHEME_CNAB2, true><<<(unsigned)nblk, 256, 0, s>>>(
-                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, c->stat_part);
+                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, c->stat_part, c->mean64);
             else
                 k_update<T, GNSS_SCHEME_RK3IF, true><<<(unsigned)nblk, 256, 0, s>>>(
-                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, c->stat_part);
+                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, c->stat_part, c->mean64);
             LAUNCH_CK(c);
             c->launches++;
             k_stats_final<<<1, STAT_SUMS * 32, 0, s>>>(c->stat_part, (int)nblk, stats_dst);
@@ -707,10 +735,10 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
         }
         if (uc.scheme == GNSS_SCHEME_CNAB2)
             k_update<T, GNSS_SCHEME_CNAB2><<<(unsigned)nblk, 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz,
-                                                                        c->ncp, uc, full_rows);
+                                                                        c->ncp, uc, full_rows, nullptr, c->mean64);
         else
             k_update<T, GNSS_SCHEME_RK3IF><<<(unsigned)nblk, 256, 0, s>>>(SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz,
-                                                                        c->ncp, uc, full_rows);
+                                                                        c->ncp, uc, full_rows, nullptr, c->mean64);
         LAUNCH_CK(c);
     }
     return GNSS_OK;
@@ -989,8 +1017,8 @@ gnss_status gnss_set_option(gnss_ctx *c, int key, int value) {
         return GNSS_OK;
     }
     if (key != GNSS_OPT_ZVARIANT && key != GNSS_OPT_PVARIANT) return fail(c, GNSS_ERR_INVALID, "unknown option %d", key);
-    const int top = key == GNSS_OPT_ZVARIANT ? GNSS_VARIANT_WARPSPEC : GNSS_VARIANT_STAGED;
-    if (value < GNSS_VARIANT_AUTO || value > top)
+    const int top = key == GNSS_OPT_ZVARIANT ? GNSS_VARIANT_WARPSPEC : GNSS_VARIANT_TENSOR;
+    if (value < GNSS_VARIANT_AUTO || value > top || (key == GNSS_OPT_PVARIANT && value == GNSS_VARIANT_WARPSPEC))
         return fail(c, GNSS_ERR_INVALID, "bad variant %d for option %d", value, key);
     (key == GNSS_OPT_ZVARIANT ? c->zvariant : c->pvariant) = value;
     return GNSS_OK;
@@ -1260,7 +1288,20 @@ gnss_status gnss_create(const gnss_config *cfg, gnss_ctx **out) {
         gnss_destroy(c);
         return GNSS_ERR_NOMEM;
     }
-    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, k.device);
+    if (k.precision == GNSS_FP32) {   // the mean-profile line in FP64 (k_update); zero: taken from the fields
+        const size_t mb = sizeof(double2) * 10 * (size_t)k.ny;
+        if (cudaMalloc(&c->mean64, mb) != cudaSuccess || cudaMemset(c->mean64, 0, mb) != cudaSuccess) {
+            cudaGetLastError();
+            gnss_destroy(c);
+            return GNSS_ERR_NOMEM;
+        }
+        c->owned_bytes += mb;
+    }
+    if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, k.device) != cudaSuccess) {
+        cudaGetLastError();
+        gnss_destroy(c);
+        return GNSS_ERR_CUDA;
+    }
     *out = c;
     return GNSS_OK;
 }
@@ -1277,6 +1318,7 @@ gnss_status gnss_destroy(gnss_ctx *c) {
     if (c->turb_dev) cudaFree(c->turb_dev);
     if (c->turb_host) cudaFreeHost(c->turb_host);
     if (c->d_err) cudaFree(c->d_err);
+    if (c->mean64) cudaFree(c->mean64);
     if (c->res) cudaFree(c->res);
     if (c->run_sums) cudaFree(c->run_sums);
     if (c->run_sums_host) cudaFreeHost(c->run_sums_host);
@@ -1693,6 +1735,8 @@ gnss_status gnss_run_host(gnss_ctx *c, const void *host_in, void *host_out, int 
     // CN/AB2 run that starts with AB2.
     const bool clear_hist = c->cfg.scheme == GNSS_SCHEME_CNAB2 && !first_euler;
     CK(c, cudaMemsetAsync(base, 0, (clear_hist ? 2 : 1) * (size_t)nf * fb, s));
+    if (c->mean64)   // a new state: its FP64 mean line starts from the uploaded values
+        CK(c, cudaMemsetAsync(c->mean64, 0, sizeof(double2) * 10 * (size_t)c->g.ny, s));
     size_t moved = 0;
     for (int q = 0; q < nf; ++q) {
         CK(c, copy_box(c, *sp[q], in + (size_t)q * fb, true, cudaMemcpyHostToDevice, s, &moved));

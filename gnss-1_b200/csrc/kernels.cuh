@@ -591,6 +591,14 @@ struct UpdCoef {
 // the history held there); modes outside the box are never touched.  Every
 // load of a mode is issued before its first store.
 //
+// With `mean` (FP32 contexts), the mean-profile line kx = kz = 0 (all kept ky;
+// the y profiles of initialize.cu:114-194 averaged by statistics.cu:1936-2003)
+// is advanced in FP64: mean[q ny + ky] holds the FP64 state of field q and
+// mean[(5 + q) ny + ky] its FP64 history.  A kept value is used when it
+// rounds to the FP32 value in the field (the field was last written by this
+// update); otherwise the field's own value is taken, so a state written
+// anew by the caller starts from what it holds.  Both copies are written.
+//
 // With STATS, the kernel also sums, over the modes it writes, the spectral
 // statistics of the new state (the six sums of k_stats_partial: the full
 // spectrum through the kz mirror, statistics.cu:1494-1845) and writes one row
@@ -601,7 +609,7 @@ template <typename T, int SCHEME, bool STATS = false>
 __global__ void __launch_bounds__(256)
 k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
          const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
-         UpdCoef c, int full_rows, double *__restrict__ partial = nullptr) {
+         UpdCoef c, int full_rows, double *__restrict__ partial = nullptr, double2 *__restrict__ mean = nullptr) {
     using V = V2<T>;
     double acc[STATS ? STAT_SUMS : 1] = {};
     const int nkx = kx_keep.count(), nky = ky_keep.count();
@@ -673,34 +681,50 @@ k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ Fiel
                 }
             }
             V sv[STATS ? 5 : 1];   // the stored new state (the statistics read these values)
+            // the mean-profile line in FP64 (FP32 contexts)
+            const bool mline = sizeof(T) == 4 && mean != nullptr && kxi == 0 && kzi == 0;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 if constexpr (STATS) sv[q] = V{T(0), T(0)};
                 if (q >= nf) break;
-                const double fr = (double)f[q].x, fi = (double)f[q].y;
+                double fr = (double)f[q].x, fi = (double)f[q].y;
+                double hr = (double)h[q].x, hi = (double)h[q].y;
+                if (mline) {
+                    const double2 sm = mean[q * g.ny + kyi];
+                    if ((T)sm.x == f[q].x && (T)sm.y == f[q].y) { fr = sm.x; fi = sm.y; }
+                    if (read_hist) {
+                        const double2 hm = mean[(5 + q) * g.ny + kyi];
+                        if ((T)hm.x == h[q].x && (T)hm.y == h[q].y) { hr = hm.x; hi = hm.y; }
+                    }
+                }
+                double nr, ni, gr, gi;   // new state and new history
                 if constexpr (SCHEME == 0) {
                     // eulerKernel_mgpu / adamsBashforthKernel_mgpu (solver.cu:547-585)
                     const double hk = c.hnum[q] * ksq;
                     const double am = 1.0 - hk;
                     const double ib = 1.0 / (1.0 + hk);
-                    double nr, ni;
                     if (c.euler) {
                         nr = (am * fr + c.dt * R[q][0]) * ib;
                         ni = (am * fi + c.dt * R[q][1]) * ib;
                     } else {
-                        nr = (am * fr + c.dt * (1.5 * R[q][0] - 0.5 * (double)h[q].x)) * ib;
-                        ni = (am * fi + c.dt * (1.5 * R[q][1] - 0.5 * (double)h[q].y)) * ib;
+                        nr = (am * fr + c.dt * (1.5 * R[q][0] - 0.5 * hr)) * ib;
+                        ni = (am * fi + c.dt * (1.5 * R[q][1] - 0.5 * hi)) * ib;
                     }
-                    state.p[q][idx] = V{(T)nr, (T)ni};
-                    if constexpr (STATS) sv[q] = V{(T)nr, (T)ni};
-                    hist.p[q][idx] = V{(T)R[q][0], (T)R[q][1]};   // updateKernel_mgpu (solver.cu:618-637)
+                    gr = R[q][0];   // updateKernel_mgpu (solver.cu:618-637)
+                    gi = R[q][1];
                 } else {
                     const double E = exp(-c.nu[q] * ksq * c.alph * c.dt);
-                    const double nr = E * (fr + c.gam * c.dt * R[q][0] + (double)h[q].x);
-                    const double ni = E * (fi + c.gam * c.dt * R[q][1] + (double)h[q].y);
-                    state.p[q][idx] = V{(T)nr, (T)ni};
-                    if constexpr (STATS) sv[q] = V{(T)nr, (T)ni};
-                    hist.p[q][idx] = V{(T)(c.zet_next * c.dt * E * R[q][0]), (T)(c.zet_next * c.dt * E * R[q][1])};
+                    nr = E * (fr + c.gam * c.dt * R[q][0] + hr);
+                    ni = E * (fi + c.gam * c.dt * R[q][1] + hi);
+                    gr = c.zet_next * c.dt * E * R[q][0];
+                    gi = c.zet_next * c.dt * E * R[q][1];
+                }
+                state.p[q][idx] = V{(T)nr, (T)ni};
+                if constexpr (STATS) sv[q] = V{(T)nr, (T)ni};
+                hist.p[q][idx] = V{(T)gr, (T)gi};
+                if (mline) {
+                    mean[q * g.ny + kyi] = double2{nr, ni};
+                    mean[(5 + q) * g.ny + kyi] = double2{gr, gi};
                 }
             }
             if constexpr (STATS) {   // sums of the stored (T) values, as k_stats_partial reads them

@@ -1,0 +1,400 @@
+// passtc.cuh -- strided x / y passes whose line transforms run on the tensor
+// cores as split-TF32 DFT-matrix GEMMs (FP32, N = 256 and 512).
+//
+// Same contract as k_passr / k_pass (PassSpec / PassPtrs: tiles of columns x N
+// rows, kept / compact rows and outer indices, up to two outputs per tile,
+// each the transform of the tile times a spectral multiplier, optional dealias
+// mask), for tiles of NB = 8 columns.  A length-N transform, N = N1 N2 with
+// N2 = 16, n = N2 n1 + n2, k = k1 + N1 k2, is
+//   step 1  Y[n2][k1] = sum_n1 x[N2 n1 + n2] W_N1^(n1 k1)         (DFT-N1 GEMM)
+//   twiddle Y[n2][k1] *= W_N^(n2 k1)
+//   step 3  X[k1 + N1 k2] = sum_n2 Y[n2][k1] W_N2^(n2 k2)         (DFT-N2 GEMM)
+// Each step is a real GEMM D = A B on tcgen05 (kind::tf32, M = 128, F32
+// accumulators in TMEM): the rows of A are the (column, n2) or (column, k1)
+// lines of the tile, its K index the real and imaginary parts of the line,
+// and B the real form [[Re W, Im W], [-Im W, Re W]] of the DFT matrix.  FP32
+// accuracy comes from three products per GEMM: with a = a_hi + a_lo (a_hi the
+// value rounded to TF32, a_lo the exact remainder, read as TF32 by the MMA)
+// and likewise b, D = a_hi b_hi + a_lo b_hi + a_hi b_lo, which leaves out only
+// a_lo b_lo (relative 2^-22).
+//
+// Per tile (and per output of a tile), 8 warps:
+//   P1  load the rows of the tile from global memory (issued one tile ahead,
+//       into registers), apply the mask and the multiplier, split, and write
+//       A1 (MN-major, 128-byte swizzle: conflict-free 16-byte stores);
+//   MMA step 1 (3 x 2N1/8 MMAs of 128 x 2N1 x 8), committed to mbarrier 0;
+//   P2  output of the previous tile while step 1 runs: D3 rows from TMEM into
+//       an output tile (in A3's shared memory) and coalesced row stores;
+//   P3  D1 rows from TMEM, twiddle, split, write A3;
+//   MMA step 3 (per 128-row M tile, 3 x 4 MMAs of 128 x 32 x 8), committed to
+//       mbarrier 1 -- it runs while P1 of the next tile builds A1.
+// Waits on the mbarriers are bounded: one that runs out sets bit 1 of *err
+// (err may be null: no report), waits (bounded) for the MMAs in flight, frees
+// the TMEM and leaves.
+//
+// Index maps (NB = 8 columns c of the tile):
+//   A1 row m1 = c + 8 n2 (128 rows), K index n1 (Re) or N1 + n1 (Im);
+//   D1 row m1 = TMEM lane, column k1 (Re) or N1 + k1 (Im);
+//   A3 M tile k1 / 16, row (k1 % 4) + 4 c + 32 ((k1 / 4) % 4), K index n2 / N2 + n2;
+//   D3 row = that, column k2 (Re) or N2 + k2 (Im), at TMEM column 2 N1 + 32 * tile.
+// The MN-major 128-byte-swizzle layout of an A operand: atoms of 8 K rows x
+// 32 M values (1024 bytes), chunk (16 bytes) i1 of row j0 stored at chunk
+// i1 ^ j0; atoms along M 1024 bytes apart (leading byte offset), K groups of 8
+// rows 4096 bytes apart (stride byte offset).  B operands are K-major without
+// swizzle: core matrices of 8 N rows x 4 K values (128 bytes), K chunks 128
+// bytes apart (leading), 8-row N groups 2 N1 * 32 bytes apart (stride).
+#pragma once
+#include "passreg.cuh"
+#include "tcgen05.cuh"
+
+namespace gnss {
+
+__host__ __device__ constexpr bool ptc_size(int n) { return n == 256 || n == 512; }
+
+template <int N> struct PTCfg {
+    static_assert(ptc_size(N), "tensor-core passes serve N = 256, 512");
+    static constexpr int NB = 8;                 // columns per tile
+    static constexpr int N2 = 16;
+    static constexpr int N1 = N / N2;            // 32 or 16
+    static constexpr int NT = 256;               // 8 warps
+    static constexpr int K1 = 2 * N1;            // step-1 K and N (Re and Im)
+    static constexpr int K3 = 2 * N2;            // step-3 K and N
+    static constexpr int MT3 = N1 * NB / 128;    // step-3 M tiles (2 or 1)
+    static constexpr int KG1 = K1 / 8, KG3 = K3 / 8;   // K groups: one MMA (K = 8) each
+    static constexpr int A1_BYTES = 128 * K1 * 4;      // one of hi / lo
+    static constexpr int A3_TILE = 128 * K3 * 4;
+    static constexpr int A3_BYTES = MT3 * A3_TILE;
+    static constexpr int B1_BYTES = K1 * K1 * 4, B3_BYTES = K3 * K3 * 4;
+    static constexpr int B1_SBO = (K1 / 4) * 128, B3_SBO = (K3 / 4) * 128;
+    static constexpr int OFF_A1H = 0, OFF_A1L = A1_BYTES;
+    static constexpr int OFF_A3H = 2 * A1_BYTES, OFF_A3L = OFF_A3H + A3_BYTES;
+    static constexpr int OFF_B1H = OFF_A3L + A3_BYTES, OFF_B1L = OFF_B1H + B1_BYTES;
+    static constexpr int OFF_B3H = OFF_B1L + B1_BYTES, OFF_B3L = OFF_B3H + B3_BYTES;
+    static constexpr int OFF_TW = OFF_B3L + B3_BYTES;  // N twiddles W_N^j (signed)
+    static constexpr int OFF_MISC = OFF_TW + N * 8;    // 2 mbarriers, TMEM address, dmax[NB]
+    static constexpr int SMEM = OFF_MISC + 128 + 1024; // + slack to align the base to 1024 bytes
+    static constexpr int LDO = NB;                     // output tile row pitch (complex), in A3's space
+    static constexpr uint32_t D1_COL = 0, D3_COL = K1;
+    static constexpr uint32_t TCOLS = (K1 + MT3 * K3) <= 64 ? 64u : 128u;
+    static_assert(N * LDO * 8 <= A3_BYTES, "output tile fits in A3");
+    static_assert(K1 + MT3 * K3 <= (int)TCOLS, "TMEM columns");
+};
+
+template <int N, int SIGN>
+__global__ void __launch_bounds__(256, N == 256 ? 2 : 1)
+k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ PassSpec sp,
+         const float2 *__restrict__ tw, unsigned *__restrict__ err) {
+    using C = PTCfg<N>;
+    using V = float2;
+    constexpr int NB = C::NB, N1 = C::N1, N2 = C::N2, NIT = N1 / 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t raw_addr = smem_u32(smem_raw);
+    const uint32_t base = (raw_addr + 1023u) & ~1023u;
+    unsigned char *sm = smem_raw + (base - raw_addr);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = sp.outer.count() * sp.ncolblk;
+    const int nitems = sp.nin * ntiles;   // < 2^31 (inputs x outer indices x column blocks)
+    int item = blockIdx.x;
+    if (item >= nitems) return;   // uniform for the block
+    V *twl = reinterpret_cast<V *>(sm + C::OFF_TW);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + C::OFF_MISC);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + C::OFF_MISC + 16);
+    int *dmax_s = reinterpret_cast<int *>(sm + C::OFF_MISC + 32);
+    V *outt = reinterpret_cast<V *>(sm + C::OFF_A3H);   // output tile (A3's space between the steps)
+
+    // ---- set-up: signed twiddles, the DFT matrices (split), barriers, TMEM
+    for (int i = tid; i < N; i += C::NT) {
+        const V t = tw[i];
+        twl[i] = SIGN < 0 ? t : V{t.x, -t.y};
+    }
+    __syncthreads();
+    auto put_b = [&](int off_h, int off_l, int sbo, int kk, int n, float val) {
+        const int o = (n & 7) * 16 + (n >> 3) * sbo + (kk & 3) * 4 + (kk >> 2) * 128;
+        float hi, lo;
+        tc::split_tf32(val, hi, lo);
+        *reinterpret_cast<float *>(sm + off_h + o) = hi;
+        *reinterpret_cast<float *>(sm + off_l + o) = lo;
+    };
+    // B[kk][n]: kk = Re / Im of the input index, n = Re / Im of the output index
+    for (int i = tid; i < C::K1 * C::K1; i += C::NT) {
+        const int kk = i / C::K1, n = i - kk * C::K1;
+        const int a = kk % N1, b = n % N1;
+        const V w = twl[(N2 * a * b) % N];   // W_N1^(a b)
+        const float v = (kk < N1) == (n < N1) ? w.x : (kk < N1 ? w.y : -w.y);
+        put_b(C::OFF_B1H, C::OFF_B1L, C::B1_SBO, kk, n, v);
+    }
+    for (int i = tid; i < C::K3 * C::K3; i += C::NT) {
+        const int kk = i / C::K3, n = i - kk * C::K3;
+        const int a = kk % N2, b = n % N2;
+        const V w = twl[(N1 * a * b) % N];   // W_N2^(a b)
+        const float v = (kk < N2) == (n < N2) ? w.x : (kk < N2 ? w.y : -w.y);
+        put_b(C::OFF_B3H, C::OFF_B3L, C::B3_SBO, kk, n, v);
+    }
+    if (warp == 0) tc::alloc(tslot, C::TCOLS);
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    fence_proxy_async_smem();   // B matrices written by threads, read by the MMAs
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const WaitCtl wc(err);
+    bool failed = false;
+
+    auto decode = [&](int it, int &fi, int &oc, int &o, int &c0) {
+        fi = it / ntiles;
+        const int t = it - fi * ntiles;
+        oc = t / sp.ncolblk;
+        o = sp.outer.expand(oc);
+        c0 = (t - oc * sp.ncolblk) * NB;
+    };
+
+    // ---- P1 geometry: rows N2 (j + 8 it) + n2 (it < NIT), columns 4 g .. 4 g + 3
+    const int pj = lane & 7, pg = (lane >> 3) & 1, pn2 = (lane >> 4) + 2 * warp;
+    V raw[NIT][4];
+    auto load = [&](int it_item) {
+        int fi, oc, o, c0;
+        decode(it_item, fi, oc, o, c0);
+        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+            const int row = N2 * (pj + 8 * it) + pn2;
+            const bool rk = sp.row_in.kept(row);
+            const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
+            const V *p = src + (long long)r * sp.s_row + 4 * pg;
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                raw[it][e] = (rk && c0 + 4 * pg + e < sp.ncols) ? __ldg(p + e) : V{0.f, 0.f};
+        }
+    };
+    // A1 from the loaded rows: mask, multiplier, split, 16-byte stores
+    auto build_a1 = [&](int mul, int c0, double k_out) {
+        const int i1 = (pg + 2 * pn2) & 7, i2 = pn2 >> 2;
+        float kc[4];
+        double kcd[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            kcd[e] = wavenum(c0 + 4 * pg + e, sp.n_col, sp.dk_col);
+            kc[e] = (float)kcd[e];
+        }
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+            const int n1 = pj + 8 * it, row = N2 * n1 + pn2;
+            const float kr = (float)sp.dk_row * (float)(row < sp.n_row / 2 ? row : row - sp.n_row);
+            float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                V x = raw[it][e];
+                if (sp.mask && row_dist<N>(row) > dmax_s[4 * pg + e]) x = V{0.f, 0.f};
+                if (mul == V_IK_ROW) {
+                    x = V{-kr * x.y, kr * x.x};
+                } else if (mul == V_IK_OUT || mul == V_IK_COL) {
+                    const float kk = mul == V_IK_OUT ? (float)k_out : kc[e];
+                    x = V{-kk * x.y, kk * x.x};
+                } else if (mul == V_LAP) {
+                    const float k2 = (float)ksq3(wavenum(row, sp.n_row, sp.dk_row), k_out, kcd[e]);
+                    x = V{-k2 * x.x, -k2 * x.y};
+                }
+                tc::split_tf32(x.x, rh[e], rl[e]);
+                tc::split_tf32(x.y, ih[e], il[e]);
+            }
+            const int sw = ((i1 ^ pj) << 4) + pj * 128 + i2 * 1024;
+            const int o_re = it * 4096 + sw, o_im = (N1 / 8 + it) * 4096 + sw;
+            *reinterpret_cast<float4 *>(sm + C::OFF_A1H + o_re) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+            *reinterpret_cast<float4 *>(sm + C::OFF_A1L + o_re) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+            *reinterpret_cast<float4 *>(sm + C::OFF_A1H + o_im) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+            *reinterpret_cast<float4 *>(sm + C::OFF_A1L + o_im) = make_float4(il[0], il[1], il[2], il[3]);
+        }
+    };
+    auto issue_step1 = [&]() {
+        tc::fence_after_sync();
+        constexpr uint32_t id = tc::idesc_tf32(128, C::K1, 1);
+#pragma unroll 1
+        for (int kg = 0; kg < C::KG1; ++kg) {
+            const uint64_t ah = tc::smem_desc(base + C::OFF_A1H + kg * 4096, 1024, 4096, tc::LAYOUT_SW128);
+            const uint64_t al = tc::smem_desc(base + C::OFF_A1L + kg * 4096, 1024, 4096, tc::LAYOUT_SW128);
+            const uint64_t bh = tc::smem_desc(base + C::OFF_B1H + kg * 256, 128, C::B1_SBO, tc::LAYOUT_NONE);
+            const uint64_t bl = tc::smem_desc(base + C::OFF_B1L + kg * 256, 128, C::B1_SBO, tc::LAYOUT_NONE);
+            tc::mma_tf32(tmem + C::D1_COL, ah, bh, id, kg > 0 ? 1u : 0u);
+            tc::mma_tf32(tmem + C::D1_COL, al, bh, id, 1u);
+            tc::mma_tf32(tmem + C::D1_COL, ah, bl, id, 1u);
+        }
+        tc::commit(&bar[0]);
+    };
+    auto issue_step3 = [&]() {
+        tc::fence_after_sync();
+        constexpr uint32_t id = tc::idesc_tf32(128, C::K3, 1);
+#pragma unroll 1
+        for (int t = 0; t < C::MT3; ++t) {
+#pragma unroll 1
+            for (int kg = 0; kg < C::KG3; ++kg) {
+                const int ao = t * C::A3_TILE + kg * 4096;
+                const uint64_t ah = tc::smem_desc(base + C::OFF_A3H + ao, 1024, 4096, tc::LAYOUT_SW128);
+                const uint64_t al = tc::smem_desc(base + C::OFF_A3L + ao, 1024, 4096, tc::LAYOUT_SW128);
+                const uint64_t bh = tc::smem_desc(base + C::OFF_B3H + kg * 256, 128, C::B3_SBO, tc::LAYOUT_NONE);
+                const uint64_t bl = tc::smem_desc(base + C::OFF_B3L + kg * 256, 128, C::B3_SBO, tc::LAYOUT_NONE);
+                const uint32_t d = tmem + C::D3_COL + t * C::K3;
+                tc::mma_tf32(d, ah, bh, id, kg > 0 ? 1u : 0u);
+                tc::mma_tf32(d, al, bh, id, 1u);
+                tc::mma_tf32(d, ah, bl, id, 1u);
+            }
+        }
+        tc::commit(&bar[1]);
+    };
+    // P3: D1 -> twiddle -> split -> A3.  Thread: TMEM lane m1 = 32 q + lane (c = lane % 8,
+    // n2 = 4 q + lane / 8), k1 in [h KH, h KH + KH)
+    auto build_a3 = [&]() {
+        constexpr int KH = N1 / 2;
+        const int q = warp & 3, h = warp >> 2;
+        const int c = lane & 7, n2 = 4 * q + (lane >> 3);
+        float yr[KH], yi[KH];
+        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D1_COL + h * KH;
+        if constexpr (KH == 16) {
+            tc::ld_x16(ta, yr);
+            tc::ld_x16(ta + N1, yi);
+        } else {
+            tc::ld_x8(ta, yr);
+            tc::ld_x8(ta + N1, yi);
+        }
+        tc::wait_ld();
+        const int j0 = n2 & 7, sw = ((c ^ j0) << 4) + j0 * 128;
+        const int o_re = (n2 >> 3) * 4096 + sw, o_im = (N2 / 8 + (n2 >> 3)) * 4096 + sw;
+#pragma unroll
+        for (int gi = 0; gi < KH / 4; ++gi) {
+            float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int i = 4 * gi + e, k1 = h * KH + i;
+                const V w = twl[(n2 * k1) % N];
+                const float a = yr[i] * w.x - yi[i] * w.y, b = yr[i] * w.y + yi[i] * w.x;
+                tc::split_tf32(a, rh[e], rl[e]);
+                tc::split_tf32(b, ih[e], il[e]);
+            }
+            const int k1b = h * KH + 4 * gi;
+            const int tb = (k1b >> 4) * C::A3_TILE + ((k1b >> 2) & 3) * 1024;
+            *reinterpret_cast<float4 *>(sm + C::OFF_A3H + tb + o_re) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+            *reinterpret_cast<float4 *>(sm + C::OFF_A3L + tb + o_re) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+            *reinterpret_cast<float4 *>(sm + C::OFF_A3H + tb + o_im) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+            *reinterpret_cast<float4 *>(sm + C::OFF_A3L + tb + o_im) = make_float4(il[0], il[1], il[2], il[3]);
+        }
+    };
+    // P2: D3 -> output tile -> rows of the destination
+    auto output = [&](V *dst, int out_cols) {
+        const int q = warp & 3, h = warp >> 2;
+        const int c = (lane >> 2) & 7;
+        if constexpr (C::MT3 == 2) {   // warp half h reads M tile h, every k2
+            const int k1 = (lane & 3) + 4 * q + 16 * h;
+            float xr[16], xi[16];
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + h * C::K3;
+            tc::ld_x16(ta, xr);
+            tc::ld_x16(ta + N2, xi);
+            tc::wait_ld();
+#pragma unroll
+            for (int k2 = 0; k2 < 16; ++k2) outt[(k1 + N1 * k2) * C::LDO + c] = V{xr[k2], xi[k2]};
+        } else {   // one M tile: warp half h reads k2 in [8 h, 8 h + 8)
+            const int k1 = (lane & 3) + 4 * q;
+            float xr[8], xi[8];
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + 8 * h;
+            tc::ld_x8(ta, xr);
+            tc::ld_x8(ta + N2, xi);
+            tc::wait_ld();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) outt[(k1 + N1 * (8 * h + i)) * C::LDO + c] = V{xr[i], xi[i]};
+        }
+        tc::fence_before_sync();
+        __syncthreads();   // output tile complete; D3 read
+        const int nrow = sp.row_out.count();
+        const int drow = (int)sp.d_row;   // row pitch of the destination (< 2^31 elements per tile)
+        const int cc = tid & 7;
+        if (cc < out_cols)
+            for (int rc = tid >> 3; rc < nrow; rc += C::NT / 8) {
+                const int row = sp.row_out.expand(rc);
+                const int r = sp.row_out_compact ? rc : row;
+                dst[r * drow + cc] = outt[row * C::LDO + cc];
+            }
+        __syncthreads();   // A3's space free again
+    };
+    auto wait_bar = [&](int b, unsigned parity) -> bool {
+        const bool ok = mbar_wait_bounded(&bar[b], parity, wc.limit);
+        return !__syncthreads_or(!ok);
+    };
+
+    // ---- the pipeline over units (tile, output)
+    unsigned unit = 0;
+    bool pend1 = false, pend3 = false;   // step 1 of `unit` / step 3 of `unit - 1` issued and not yet awaited
+    V *prev_dst = nullptr;
+    int prev_cols = 0;
+    load(item);
+    while (item < nitems && !failed) {
+        int fi, oc, o, c0;
+        decode(item, fi, oc, o, c0);
+        const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
+        if (sp.mask) {   // rows kept by the dealias mask in column `warp`: |row index| <= dmax
+            const double kc = wavenum(c0 + warp, sp.n_col, sp.dk_col);
+            int cnt = 0;
+            for (int d0 = 0; d0 <= N / 2; d0 += 32) {
+                const int d = d0 + lane;
+                const bool ok = d <= N / 2 && !(ksq3(sp.dk_row * (double)d, k_out, kc) > sp.kmax2);
+                cnt += __popc(__ballot_sync(0xffffffffu, ok));
+            }
+            if (lane == 0) dmax_s[warp] = cnt - 1;
+            __syncthreads();
+        }
+        const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const int out_cols = sp.out_ncols - c0 < NB ? sp.out_ncols - c0 : NB;
+        const int nv = sp.nvar[fi];
+        const int next = item + gridDim.x;
+        for (int v = 0; v < nv; ++v) {
+            build_a1(sp.vmul[fi][v], c0, k_out);
+            if (v + 1 == nv && next < nitems) load(next);   // the rows of the next tile, in flight meanwhile
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0) issue_step1();
+            pend1 = true;
+            if (pend3) {   // output of the previous unit while step 1 runs
+                if (!wait_bar(1, (unit - 1) & 1u)) { failed = true; break; }
+                pend3 = false;
+                tc::fence_after_sync();
+                output(prev_dst, prev_cols);
+            }
+            if (!wait_bar(0, unit & 1u)) { failed = true; break; }
+            pend1 = false;
+            tc::fence_after_sync();
+            build_a3();
+            fence_proxy_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();
+            if (tid == 0) issue_step3();
+            pend3 = true;
+            prev_dst = P.out[sp.vout[fi][v]] + dbase;
+            prev_cols = out_cols;
+            ++unit;
+        }
+        item = next;
+    }
+    if (!failed && pend3) {
+        if (wait_bar(1, (unit - 1) & 1u)) {
+            pend3 = false;
+            tc::fence_after_sync();
+            output(prev_dst, prev_cols);
+        } else {
+            failed = true;
+        }
+    }
+    if (failed) {   // let the MMAs in flight finish (bounded) before the TMEM is freed
+        if (tid == 0 && err) atomicOr(err, 2u);
+        if (pend3) mbar_wait_bounded(&bar[1], (unit - 1) & 1u, wc.limit);
+        if (pend1) mbar_wait_bounded(&bar[0], unit & 1u, wc.limit);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::dealloc(tmem, C::TCOLS);
+    }
+}
+
+}  // namespace gnss

@@ -41,6 +41,7 @@ GNSS_VARIANT_AUTO = GNSS_ZVARIANT_AUTO = 0
 GNSS_VARIANT_REGISTER = GNSS_ZVARIANT_REGISTER = 1
 GNSS_VARIANT_STAGED = GNSS_ZVARIANT_STAGED = 2
 GNSS_VARIANT_WARPSPEC = 3   # GNSS_OPT_ZVARIANT only
+GNSS_VARIANT_TENSOR = 4     # GNSS_OPT_PVARIANT only: split-TF32 DFT-GEMM passes on tcgen05 (FP32, N = 256, 512)
 STAT_NAMES = ("ke", "vrms2", "eps", "chi_s", "chi_c", "var_s", "var_c")
 SUPPORTED_SIZES = (8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512)
 

@@ -252,8 +252,15 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  *   GNSS_VARIANT_WARPSPEC  (GNSS_OPT_ZVARIANT only) the register z kernel
  *                          with separate inverse and forward warps, where it
  *                          exists (FP32, one scalar, no colloid term, z
- *                          length 256 or 512); the register kernel otherwise.
- * Every variant computes the same step to round-off. */
+ *                          length 256 or 512); the register kernel otherwise;
+ *   GNSS_VARIANT_TENSOR    (GNSS_OPT_PVARIANT only) line transforms on the
+ *                          tensor cores as split-TF32 DFT-matrix GEMMs
+ *                          (tcgen05, three TF32 products per GEMM with FP32
+ *                          accumulation) where they exist: FP32, x / y
+ *                          lengths 256 and 512; the AUTO choice elsewhere.
+ * Every variant computes the same step to round-off (the tensor-core
+ * variant to FP32 accuracy: it replaces the butterflies' rounding with the
+ * 2^-22 relative error of the split products). */
 #define GNSS_OPT_ZVARIANT 0
 #define GNSS_OPT_PVARIANT 1
 #define GNSS_OPT_ZKERNEL 2   /* read-only (gnss_get_option): the z kernel the options select for this
@@ -268,6 +275,7 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
 #define GNSS_VARIANT_REGISTER 1
 #define GNSS_VARIANT_STAGED 2
 #define GNSS_VARIANT_WARPSPEC 3
+#define GNSS_VARIANT_TENSOR 4
 #define GNSS_ZVARIANT_AUTO GNSS_VARIANT_AUTO
 #define GNSS_ZVARIANT_REGISTER GNSS_VARIANT_REGISTER
 #define GNSS_ZVARIANT_STAGED GNSS_VARIANT_STAGED

@@ -213,6 +213,12 @@ def test_mixed_precision_config3_128(torch_cuda):
     for q, name in enumerate("uvws"):
         err = rel_l2(out[G.GNSS_FP32][q].astype(np.complex128), out[G.GNSS_FP64][q])
         assert err < 1e-5, f"{name}: rel L2 {err:.3e} after {steps} steps"
+    # the mean profiles (the kx = kz = 0 line, kept in FP64 by the update): only the FP32 nonlinear
+    # term's contribution to them differs from the FP64 step
+    for q, name in ((0, "u"), (3, "s")):
+        err = rel_l2(out[G.GNSS_FP32][q][:, 0, 0].astype(np.complex128), out[G.GNSS_FP64][q][:, 0, 0])
+        print(f"mean profile {name}: rel L2 {err:.3e}")
+        assert err < 1e-8, f"mean profile {name}: rel L2 {err:.3e} after {steps} steps"
 
 
 @pytest.mark.gpu
