@@ -21,7 +21,7 @@
 // Per tile (and per output of a tile), 8 warps:
 //   P1  load the rows of the tile from global memory (issued one tile ahead,
 //       into registers), apply the mask and the multiplier, split, and write
-//       A1 (MN-major, 128-byte swizzle: conflict-free 16-byte stores);
+//       A1 (16-byte stores of 4 consecutive n1);
 //   MMA step 1 (3 x 2N1/8 MMAs of 128 x 2N1 x 8), committed to mbarrier 0;
 //   P2  output of the previous tile while step 1 runs: D3 rows from TMEM into
 //       an output tile (in A3's shared memory) and coalesced row stores;
@@ -35,14 +35,15 @@
 // Index maps (NB = 8 columns c of the tile):
 //   A1 row m1 = c + 8 n2 (128 rows), K index n1 (Re) or N1 + n1 (Im);
 //   D1 row m1 = TMEM lane, column k1 (Re) or N1 + k1 (Im);
-//   A3 M tile k1 / 16, row (k1 % 4) + 4 c + 32 ((k1 / 4) % 4), K index n2 / N2 + n2;
+//   A3 M tile k1 / 16, row c + 8 (k1 % 16), K index n2 (Re) or N2 + n2 (Im);
 //   D3 row = that, column k2 (Re) or N2 + k2 (Im), at TMEM column 2 N1 + 32 * tile.
-// The MN-major 128-byte-swizzle layout of an A operand: atoms of 8 K rows x
-// 32 M values (1024 bytes), chunk (16 bytes) i1 of row j0 stored at chunk
-// i1 ^ j0; atoms along M 1024 bytes apart (leading byte offset), K groups of 8
-// rows 4096 bytes apart (stride byte offset).  B operands are K-major without
-// swizzle: core matrices of 8 N rows x 4 K values (128 bytes), K chunks 128
-// bytes apart (leading), 8-row N groups 2 N1 * 32 bytes apart (stride).
+// Operands are K-major without swizzle: core matrices of 8 rows x 4 K values
+// (128 bytes, a row's 16 bytes contiguous), the K chunks of a core-matrix row
+// group 128 bytes apart (leading byte offset), row groups K * 4 * 4 bytes apart
+// (stride byte offset); an MMA (K = 8) reads two chunks.  Row r % 8 of a core
+// matrix is 16 bytes at (r % 8) * 16, so the 8 lanes that own the 8 columns of
+// the tile (A1, 16-byte stores) or, with the column and n2 % 4, the 32 words
+// of a row group's chunk (A3, 4-byte stores) hit distinct banks.
 #pragma once
 #include "passreg.cuh"
 #include "tcgen05.cuh"
@@ -66,6 +67,7 @@ template <int N> struct PTCfg {
     static constexpr int A3_BYTES = MT3 * A3_TILE;
     static constexpr int B1_BYTES = K1 * K1 * 4, B3_BYTES = K3 * K3 * 4;
     static constexpr int B1_SBO = (K1 / 4) * 128, B3_SBO = (K3 / 4) * 128;
+    static constexpr int A1_SBO = B1_SBO, A3_SBO = B3_SBO;   // row-group strides of the A operands
     static constexpr int OFF_A1H = 0, OFF_A1L = A1_BYTES;
     static constexpr int OFF_A3H = 2 * A1_BYTES, OFF_A3L = OFF_A3H + A3_BYTES;
     static constexpr int OFF_B1H = OFF_A3L + A3_BYTES, OFF_B1L = OFF_B1H + B1_BYTES;
@@ -152,57 +154,54 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         c0 = (t - oc * sp.ncolblk) * NB;
     };
 
-    // ---- P1 geometry: rows N2 (j + 8 it) + n2 (it < NIT), columns 4 g .. 4 g + 3
-    const int pj = lane & 7, pg = (lane >> 3) & 1, pn2 = (lane >> 4) + 2 * warp;
+    // ---- P1 geometry: column c, rows N2 (4 a + e) + n2 (e < 4) for a = (warp >> 2) + 2 it, it < NIT
+    const int pc = lane & 7, pn2 = (lane >> 3) + 4 * (warp & 3), pa0 = warp >> 2;
     V raw[NIT][4];
     auto load = [&](int it_item) {
         int fi, oc, o, c0;
         decode(it_item, fi, oc, o, c0);
-        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0 + pc;
+        const bool col_ok = c0 + pc < sp.ncols;
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
-            const int row = N2 * (pj + 8 * it) + pn2;
-            const bool rk = sp.row_in.kept(row);
-            const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
-            const V *p = src + (long long)r * sp.s_row + 4 * pg;
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
-                raw[it][e] = (rk && c0 + 4 * pg + e < sp.ncols) ? __ldg(p + e) : V{0.f, 0.f};
+            for (int e = 0; e < 4; ++e) {
+                const int row = N2 * (4 * (pa0 + 2 * it) + e) + pn2;
+                const bool rk = col_ok && sp.row_in.kept(row);
+                const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
+                raw[it][e] = rk ? __ldg(src + (long long)r * sp.s_row) : V{0.f, 0.f};
+            }
         }
     };
-    // A1 from the loaded rows: mask, multiplier, split, 16-byte stores
+    // A1 from the loaded rows: mask, multiplier, split, 16-byte stores (4 consecutive n1 of row m1 = c + 8 n2)
     auto build_a1 = [&](int mul, int c0, double k_out) {
-        const int i1 = (pg + 2 * pn2) & 7, i2 = pn2 >> 2;
-        float kc[4];
-        double kcd[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            kcd[e] = wavenum(c0 + 4 * pg + e, sp.n_col, sp.dk_col);
-            kc[e] = (float)kcd[e];
-        }
+        const double kcd = wavenum(c0 + pc, sp.n_col, sp.dk_col);
+        const float kc = (float)kcd;
+        const int dmax = sp.mask ? dmax_s[pc] : N;
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
-            const int n1 = pj + 8 * it, row = N2 * n1 + pn2;
-            const float kr = (float)sp.dk_row * (float)(row < sp.n_row / 2 ? row : row - sp.n_row);
+            const int a = pa0 + 2 * it;
             float rh[4], rl[4], ih[4], il[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
+                const int row = N2 * (4 * a + e) + pn2;
                 V x = raw[it][e];
-                if (sp.mask && row_dist<N>(row) > dmax_s[4 * pg + e]) x = V{0.f, 0.f};
+                if (row_dist<N>(row) > dmax) x = V{0.f, 0.f};
                 if (mul == V_IK_ROW) {
+                    const float kr = (float)sp.dk_row * (float)(row < sp.n_row / 2 ? row : row - sp.n_row);
                     x = V{-kr * x.y, kr * x.x};
                 } else if (mul == V_IK_OUT || mul == V_IK_COL) {
-                    const float kk = mul == V_IK_OUT ? (float)k_out : kc[e];
+                    const float kk = mul == V_IK_OUT ? (float)k_out : kc;
                     x = V{-kk * x.y, kk * x.x};
                 } else if (mul == V_LAP) {
-                    const float k2 = (float)ksq3(wavenum(row, sp.n_row, sp.dk_row), k_out, kcd[e]);
+                    const float k2 = (float)ksq3(wavenum(row, sp.n_row, sp.dk_row), k_out, kcd);
                     x = V{-k2 * x.x, -k2 * x.y};
                 }
                 tc::split_tf32(x.x, rh[e], rl[e]);
                 tc::split_tf32(x.y, ih[e], il[e]);
             }
-            const int sw = ((i1 ^ pj) << 4) + pj * 128 + i2 * 1024;
-            const int o_re = it * 4096 + sw, o_im = (N1 / 8 + it) * 4096 + sw;
+            const int o_re = pc * 16 + pn2 * C::A1_SBO + a * 128;
+            const int o_im = o_re + (N1 / 4) * 128;
             *reinterpret_cast<float4 *>(sm + C::OFF_A1H + o_re) = make_float4(rh[0], rh[1], rh[2], rh[3]);
             *reinterpret_cast<float4 *>(sm + C::OFF_A1L + o_re) = make_float4(rl[0], rl[1], rl[2], rl[3]);
             *reinterpret_cast<float4 *>(sm + C::OFF_A1H + o_im) = make_float4(ih[0], ih[1], ih[2], ih[3]);
@@ -211,11 +210,11 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     };
     auto issue_step1 = [&]() {
         tc::fence_after_sync();
-        constexpr uint32_t id = tc::idesc_tf32(128, C::K1, 1);
+        constexpr uint32_t id = tc::idesc_tf32(128, C::K1, 0);
 #pragma unroll 1
         for (int kg = 0; kg < C::KG1; ++kg) {
-            const uint64_t ah = tc::smem_desc(base + C::OFF_A1H + kg * 4096, 1024, 4096, tc::LAYOUT_SW128);
-            const uint64_t al = tc::smem_desc(base + C::OFF_A1L + kg * 4096, 1024, 4096, tc::LAYOUT_SW128);
+            const uint64_t ah = tc::smem_desc(base + C::OFF_A1H + kg * 256, 128, C::A1_SBO, tc::LAYOUT_NONE);
+            const uint64_t al = tc::smem_desc(base + C::OFF_A1L + kg * 256, 128, C::A1_SBO, tc::LAYOUT_NONE);
             const uint64_t bh = tc::smem_desc(base + C::OFF_B1H + kg * 256, 128, C::B1_SBO, tc::LAYOUT_NONE);
             const uint64_t bl = tc::smem_desc(base + C::OFF_B1L + kg * 256, 128, C::B1_SBO, tc::LAYOUT_NONE);
             tc::mma_tf32(tmem + C::D1_COL, ah, bh, id, kg > 0 ? 1u : 0u);
@@ -226,14 +225,14 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     };
     auto issue_step3 = [&]() {
         tc::fence_after_sync();
-        constexpr uint32_t id = tc::idesc_tf32(128, C::K3, 1);
+        constexpr uint32_t id = tc::idesc_tf32(128, C::K3, 0);
 #pragma unroll 1
         for (int t = 0; t < C::MT3; ++t) {
 #pragma unroll 1
             for (int kg = 0; kg < C::KG3; ++kg) {
-                const int ao = t * C::A3_TILE + kg * 4096;
-                const uint64_t ah = tc::smem_desc(base + C::OFF_A3H + ao, 1024, 4096, tc::LAYOUT_SW128);
-                const uint64_t al = tc::smem_desc(base + C::OFF_A3L + ao, 1024, 4096, tc::LAYOUT_SW128);
+                const int ao = t * C::A3_TILE + kg * 256;
+                const uint64_t ah = tc::smem_desc(base + C::OFF_A3H + ao, 128, C::A3_SBO, tc::LAYOUT_NONE);
+                const uint64_t al = tc::smem_desc(base + C::OFF_A3L + ao, 128, C::A3_SBO, tc::LAYOUT_NONE);
                 const uint64_t bh = tc::smem_desc(base + C::OFF_B3H + kg * 256, 128, C::B3_SBO, tc::LAYOUT_NONE);
                 const uint64_t bl = tc::smem_desc(base + C::OFF_B3L + kg * 256, 128, C::B3_SBO, tc::LAYOUT_NONE);
                 const uint32_t d = tmem + C::D3_COL + t * C::K3;
@@ -245,7 +244,7 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         tc::commit(&bar[1]);
     };
     // P3: D1 -> twiddle -> split -> A3.  Thread: TMEM lane m1 = 32 q + lane (c = lane % 8,
-    // n2 = 4 q + lane / 8), k1 in [h KH, h KH + KH)
+    // n2 = 4 q + lane / 8), k1 in [h KH, h KH + KH); 4-byte stores into rows c + 8 (k1 % 16)
     auto build_a3 = [&]() {
         constexpr int KH = N1 / 2;
         const int q = warp & 3, h = warp >> 2;
@@ -260,33 +259,29 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
             tc::ld_x8(ta + N1, yi);
         }
         tc::wait_ld();
-        const int j0 = n2 & 7, sw = ((c ^ j0) << 4) + j0 * 128;
-        const int o_re = (n2 >> 3) * 4096 + sw, o_im = (N2 / 8 + (n2 >> 3)) * 4096 + sw;
+        const int o_re = c * 16 + (n2 >> 2) * 128 + (n2 & 3) * 4;
+        const int o_im = o_re + (N2 / 4) * 128;
 #pragma unroll
-        for (int gi = 0; gi < KH / 4; ++gi) {
-            float rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int i = 4 * gi + e, k1 = h * KH + i;
-                const V w = twl[(n2 * k1) % N];
-                const float a = yr[i] * w.x - yi[i] * w.y, b = yr[i] * w.y + yi[i] * w.x;
-                tc::split_tf32(a, rh[e], rl[e]);
-                tc::split_tf32(b, ih[e], il[e]);
-            }
-            const int k1b = h * KH + 4 * gi;
-            const int tb = (k1b >> 4) * C::A3_TILE + ((k1b >> 2) & 3) * 1024;
-            *reinterpret_cast<float4 *>(sm + C::OFF_A3H + tb + o_re) = make_float4(rh[0], rh[1], rh[2], rh[3]);
-            *reinterpret_cast<float4 *>(sm + C::OFF_A3L + tb + o_re) = make_float4(rl[0], rl[1], rl[2], rl[3]);
-            *reinterpret_cast<float4 *>(sm + C::OFF_A3H + tb + o_im) = make_float4(ih[0], ih[1], ih[2], ih[3]);
-            *reinterpret_cast<float4 *>(sm + C::OFF_A3L + tb + o_im) = make_float4(il[0], il[1], il[2], il[3]);
+        for (int i = 0; i < KH; ++i) {
+            const int k1 = h * KH + i;
+            const V w = twl[(n2 * k1) % N];
+            const float a = yr[i] * w.x - yi[i] * w.y, b = yr[i] * w.y + yi[i] * w.x;
+            float rh, rl, ih, il;
+            tc::split_tf32(a, rh, rl);
+            tc::split_tf32(b, ih, il);
+            const int rb = (k1 >> 4) * C::A3_TILE + (k1 & 15) * C::A3_SBO;
+            *reinterpret_cast<float *>(sm + C::OFF_A3H + rb + o_re) = rh;
+            *reinterpret_cast<float *>(sm + C::OFF_A3L + rb + o_re) = rl;
+            *reinterpret_cast<float *>(sm + C::OFF_A3H + rb + o_im) = ih;
+            *reinterpret_cast<float *>(sm + C::OFF_A3L + rb + o_im) = il;
         }
     };
     // P2: D3 -> output tile -> rows of the destination
     auto output = [&](V *dst, int out_cols) {
         const int q = warp & 3, h = warp >> 2;
-        const int c = (lane >> 2) & 7;
+        const int c = lane & 7;
         if constexpr (C::MT3 == 2) {   // warp half h reads M tile h, every k2
-            const int k1 = (lane & 3) + 4 * q + 16 * h;
+            const int k1 = (lane >> 3) + 4 * q + 16 * h;
             float xr[16], xi[16];
             const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + h * C::K3;
             tc::ld_x16(ta, xr);
@@ -295,7 +290,7 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
 #pragma unroll
             for (int k2 = 0; k2 < 16; ++k2) outt[(k1 + N1 * k2) * C::LDO + c] = V{xr[k2], xi[k2]};
         } else {   // one M tile: warp half h reads k2 in [8 h, 8 h + 8)
-            const int k1 = (lane & 3) + 4 * q;
+            const int k1 = (lane >> 3) + 4 * q;
             float xr[8], xi[8];
             const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + 8 * h;
             tc::ld_x8(ta, xr);

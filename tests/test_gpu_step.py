@@ -195,30 +195,36 @@ def test_run_host_matches_device_steps(torch_cuda, shape, scheme, precision, ns,
 def test_mixed_precision_config3_128(torch_cuda):
     """The mixed-precision form with the 512^3 jet's parameters (Re 5000, Sc 0.7,
     dt 2.5e-4, one scalar, noise |k| <= 8 rms 0.05) at 128^3: every field within
-    1e-5 relative L2 of the FP64 step after 100 steps from the same state."""
+    1e-5 relative L2 of the FP64 step after 100 steps from the same state.
+
+    The mean profiles (the kx = kz = 0 line, which FP32 contexts advance in
+    FP64) are compared with an FP64 run from the FP32-rounded initial state:
+    only the FP32 nonlinear term's contribution to them differs, so they agree
+    far below the FP32 rounding of the state (6e-8)."""
     import gnss_b200 as G
     torch = torch_cuda
     n, re, sc, dt, steps = 128, 5000.0, 0.7, 2.5e-4, 100
     init = G.jet_initial_state(n, n_scalars=1, seed=0, noise_kmax=8.0, amp=0.05)
+    init32 = [a.astype(np.complex64) for a in init]
+    runs = {"fp64": (G.GNSS_FP64, init), "fp64_from32": (G.GNSS_FP64, [a.astype(np.complex128) for a in init32]),
+            "fp32": (G.GNSS_FP32, init32)}
     out = {}
-    for prec, cdt in ((G.GNSS_FP64, np.complex128), (G.GNSS_FP32, np.complex64)):
+    for key, (prec, start) in runs.items():
         with G.Context(n, re=re, sc=sc, dt=dt, n_scalars=1, precision=prec) as ctx:
-            st = [to_dev(torch, a.astype(cdt)) for a in init]
+            st = [to_dev(torch, a) for a in start]
             hi = [torch.zeros_like(st[0]) for _ in st]
             ctx.de_alias(st)
             for s in range(steps):
                 ctx.solver_ps(st, hi, euler=(s == 0))
             ctx.check()
-            out[prec] = [to_host(t) for t in st]
+            out[key] = [to_host(t).astype(np.complex128) for t in st]
     for q, name in enumerate("uvws"):
-        err = rel_l2(out[G.GNSS_FP32][q].astype(np.complex128), out[G.GNSS_FP64][q])
+        err = rel_l2(out["fp32"][q], out["fp64"][q])
         assert err < 1e-5, f"{name}: rel L2 {err:.3e} after {steps} steps"
-    # the mean profiles (the kx = kz = 0 line, kept in FP64 by the update): only the FP32 nonlinear
-    # term's contribution to them differs from the FP64 step
     for q, name in ((0, "u"), (3, "s")):
-        err = rel_l2(out[G.GNSS_FP32][q][:, 0, 0].astype(np.complex128), out[G.GNSS_FP64][q][:, 0, 0])
-        print(f"mean profile {name}: rel L2 {err:.3e}")
-        assert err < 1e-8, f"mean profile {name}: rel L2 {err:.3e} after {steps} steps"
+        err = rel_l2(out["fp32"][q][:, 0, 0], out["fp64_from32"][q][:, 0, 0])
+        print(f"mean profile {name}: rel L2 {err:.3e} (against FP64 from the same FP32 state)")
+        assert err < 1e-9, f"mean profile {name}: rel L2 {err:.3e} after {steps} steps"
 
 
 @pytest.mark.gpu
