@@ -18,7 +18,7 @@
 // and likewise b, D = a_hi b_hi + a_lo b_hi + a_hi b_lo, which leaves out only
 // a_lo b_lo (relative 2^-22).
 //
-// Per tile (and per output of a tile), 8 warps:
+// Per tile (and per output of a tile), 16 warps:
 //   P1  load the rows of the tile from global memory (issued one tile ahead,
 //       into registers), apply the mask and the multiplier, split, and write
 //       A1 (16-byte stores of 4 consecutive n1);
@@ -48,6 +48,8 @@
 #include "passreg.cuh"
 #include "tcgen05.cuh"
 
+#include <type_traits>
+
 namespace gnss {
 
 __host__ __device__ constexpr bool ptc_size(int n) { return n == 256 || n == 512; }
@@ -57,7 +59,7 @@ template <int N> struct PTCfg {
     static constexpr int NB = 8;                 // columns per tile
     static constexpr int N2 = 16;
     static constexpr int N1 = N / N2;            // 32 or 16
-    static constexpr int NT = 256;               // 8 warps
+    static constexpr int NT = 512;               // 16 warps
     static constexpr int K1 = 2 * N1;            // step-1 K and N (Re and Im)
     static constexpr int K3 = 2 * N2;            // step-3 K and N
     static constexpr int MT3 = N1 * NB / 128;    // step-3 M tiles (2 or 1)
@@ -74,21 +76,24 @@ template <int N> struct PTCfg {
     static constexpr int OFF_B3H = OFF_B1L + B1_BYTES, OFF_B3L = OFF_B3H + B3_BYTES;
     static constexpr int OFF_TW = OFF_B3L + B3_BYTES;  // N twiddles W_N^j (signed)
     static constexpr int OFF_MISC = OFF_TW + N * 8;    // 2 mbarriers, TMEM address, dmax[NB]
-    static constexpr int SMEM = OFF_MISC + 128 + 1024; // + slack to align the base to 1024 bytes
+    static constexpr int OFF_OROW = OFF_MISC + 64;     // N destination row offsets
+    static constexpr int SMEM = OFF_OROW + N * 4 + 1024;   // + slack to align the base to 1024 bytes
     static constexpr int LDO = NB;                     // output tile row pitch (complex), in A3's space
     static constexpr uint32_t D1_COL = 0, D3_COL = K1;
     static constexpr uint32_t TCOLS = (K1 + MT3 * K3) <= 64 ? 64u : 128u;
+    static constexpr int NIT = N1 / 16;                // P1: groups of 4 rows per thread
+    static constexpr int KQ = N1 / 4;                  // P3: k1 per thread
     static_assert(N * LDO * 8 <= A3_BYTES, "output tile fits in A3");
     static_assert(K1 + MT3 * K3 <= (int)TCOLS, "TMEM columns");
 };
 
 template <int N, int SIGN>
-__global__ void __launch_bounds__(256, N == 256 ? 2 : 1)
+__global__ void __launch_bounds__(512, 1)
 k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ PassSpec sp,
          const float2 *__restrict__ tw, unsigned *__restrict__ err) {
     using C = PTCfg<N>;
     using V = float2;
-    constexpr int NB = C::NB, N1 = C::N1, N2 = C::N2, NIT = N1 / 8;
+    constexpr int NB = C::NB, N1 = C::N1, N2 = C::N2, NIT = C::NIT, KQ = C::KQ;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
     const uint32_t base = (raw_addr + 1023u) & ~1023u;
@@ -102,12 +107,16 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + C::OFF_MISC);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + C::OFF_MISC + 16);
     int *dmax_s = reinterpret_cast<int *>(sm + C::OFF_MISC + 32);
+    int *orow = reinterpret_cast<int *>(sm + C::OFF_OROW);
     V *outt = reinterpret_cast<V *>(sm + C::OFF_A3H);   // output tile (A3's space between the steps)
 
-    // ---- set-up: signed twiddles, the DFT matrices (split), barriers, TMEM
+    // ---- set-up: signed twiddles, the DFT matrices (split), destination rows, barriers, TMEM
     for (int i = tid; i < N; i += C::NT) {
         const V t = tw[i];
         twl[i] = SIGN < 0 ? t : V{t.x, -t.y};
+        int o = -1;   // destination offset of output row i (elements; < 2^31 per tile)
+        if (sp.row_out.kept(i)) o = (sp.row_out_compact ? sp.row_out.compact(i) : i) * (int)sp.d_row;
+        orow[i] = o;
     }
     __syncthreads();
     auto put_b = [&](int off_h, int off_l, int sbo, int kk, int n, float val) {
@@ -144,7 +153,6 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
     const WaitCtl wc(err);
-    bool failed = false;
 
     auto decode = [&](int it, int &fi, int &oc, int &o, int &c0) {
         fi = it / ntiles;
@@ -154,8 +162,18 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         c0 = (t - oc * sp.ncolblk) * NB;
     };
 
-    // ---- P1 geometry: column c, rows N2 (4 a + e) + n2 (e < 4) for a = (warp >> 2) + 2 it, it < NIT
+    // ---- P1 geometry: column pc, rows N2 (4 a + e) + pn2 (e < 4) for a = pa0 + 4 it, it < NIT.
+    // The source offsets of these rows (r s_row, or -1 where the spec keeps no row) are fixed for the launch.
     const int pc = lane & 7, pn2 = (lane >> 3) + 4 * (warp & 3), pa0 = warp >> 2;
+    int roff[NIT][4];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int row = N2 * (4 * (pa0 + 4 * it) + e) + pn2;
+            roff[it][e] = sp.row_in.kept(row) ? (sp.row_in_compact ? sp.row_in.compact(row) : row) * (int)sp.s_row
+                                              : -1;
+        }
     V raw[NIT][4];
     auto load = [&](int it_item) {
         int fi, oc, o, c0;
@@ -163,38 +181,35 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0 + pc;
         const bool col_ok = c0 + pc < sp.ncols;
 #pragma unroll
-        for (int it = 0; it < NIT; ++it) {
+        for (int it = 0; it < NIT; ++it)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int row = N2 * (4 * (pa0 + 2 * it) + e) + pn2;
-                const bool rk = col_ok && sp.row_in.kept(row);
-                const int r = sp.row_in_compact ? sp.row_in.compact(row) : row;
-                raw[it][e] = rk ? __ldg(src + (long long)r * sp.s_row) : V{0.f, 0.f};
-            }
-        }
+            for (int e = 0; e < 4; ++e)
+                raw[it][e] = (col_ok && roff[it][e] >= 0) ? __ldg(src + roff[it][e]) : V{0.f, 0.f};
     };
-    // A1 from the loaded rows: mask, multiplier, split, 16-byte stores (4 consecutive n1 of row m1 = c + 8 n2)
-    auto build_a1 = [&](int mul, int c0, double k_out) {
-        const double kcd = wavenum(c0 + pc, sp.n_col, sp.dk_col);
-        const float kc = (float)kcd;
+    // A1 from the loaded rows: mask, multiplier (fixed per output), split, 16-byte stores of 4 consecutive n1
+    // of row m1 = pc + 8 pn2
+    auto build_a1_mul = [&](auto mulc, int c0, double k_out) {
+        constexpr int MUL = decltype(mulc)::value;
         const int dmax = sp.mask ? dmax_s[pc] : N;
+        const double kcd = wavenum(c0 + pc, sp.n_col, sp.dk_col);
+        const float kk = MUL == V_IK_OUT ? (float)k_out : (float)kcd;
+        const float dkr = (float)sp.dk_row;
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
-            const int a = pa0 + 2 * it;
+            const int a = pa0 + 4 * it;
             float rh[4], rl[4], ih[4], il[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int row = N2 * (4 * a + e) + pn2;
                 V x = raw[it][e];
                 if (row_dist<N>(row) > dmax) x = V{0.f, 0.f};
-                if (mul == V_IK_ROW) {
-                    const float kr = (float)sp.dk_row * (float)(row < sp.n_row / 2 ? row : row - sp.n_row);
+                if constexpr (MUL == V_IK_ROW) {
+                    const float kr = dkr * (float)(row < N / 2 ? row : row - N);
                     x = V{-kr * x.y, kr * x.x};
-                } else if (mul == V_IK_OUT || mul == V_IK_COL) {
-                    const float kk = mul == V_IK_OUT ? (float)k_out : kc;
+                } else if constexpr (MUL == V_IK_OUT || MUL == V_IK_COL) {
                     x = V{-kk * x.y, kk * x.x};
-                } else if (mul == V_LAP) {
-                    const float k2 = (float)ksq3(wavenum(row, sp.n_row, sp.dk_row), k_out, kcd);
+                } else if constexpr (MUL == V_LAP) {
+                    const float k2 = (float)ksq3(wavenum(row, N, sp.dk_row), k_out, kcd);
                     x = V{-k2 * x.x, -k2 * x.y};
                 }
                 tc::split_tf32(x.x, rh[e], rl[e]);
@@ -206,6 +221,15 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
             *reinterpret_cast<float4 *>(sm + C::OFF_A1L + o_re) = make_float4(rl[0], rl[1], rl[2], rl[3]);
             *reinterpret_cast<float4 *>(sm + C::OFF_A1H + o_im) = make_float4(ih[0], ih[1], ih[2], ih[3]);
             *reinterpret_cast<float4 *>(sm + C::OFF_A1L + o_im) = make_float4(il[0], il[1], il[2], il[3]);
+        }
+    };
+    auto build_a1 = [&](int mul, int c0, double k_out) {
+        switch (mul) {
+            case V_IK_ROW: build_a1_mul(std::integral_constant<int, V_IK_ROW>{}, c0, k_out); break;
+            case V_IK_OUT: build_a1_mul(std::integral_constant<int, V_IK_OUT>{}, c0, k_out); break;
+            case V_IK_COL: build_a1_mul(std::integral_constant<int, V_IK_COL>{}, c0, k_out); break;
+            case V_LAP: build_a1_mul(std::integral_constant<int, V_LAP>{}, c0, k_out); break;
+            default: build_a1_mul(std::integral_constant<int, V_ONE>{}, c0, k_out); break;
         }
     };
     auto issue_step1 = [&]() {
@@ -244,27 +268,26 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         tc::commit(&bar[1]);
     };
     // P3: D1 -> twiddle -> split -> A3.  Thread: TMEM lane m1 = 32 q + lane (c = lane % 8,
-    // n2 = 4 q + lane / 8), k1 in [h KH, h KH + KH); 4-byte stores into rows c + 8 (k1 % 16)
+    // n2 = 4 q + lane / 8), k1 in [part KQ, part KQ + KQ); 4-byte stores into rows c + 8 (k1 % 16)
     auto build_a3 = [&]() {
-        constexpr int KH = N1 / 2;
-        const int q = warp & 3, h = warp >> 2;
+        const int q = warp & 3, part = warp >> 2;
         const int c = lane & 7, n2 = 4 * q + (lane >> 3);
-        float yr[KH], yi[KH];
-        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D1_COL + h * KH;
-        if constexpr (KH == 16) {
-            tc::ld_x16(ta, yr);
-            tc::ld_x16(ta + N1, yi);
-        } else {
+        float yr[KQ], yi[KQ];
+        const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D1_COL + part * KQ;
+        if constexpr (KQ == 8) {
             tc::ld_x8(ta, yr);
             tc::ld_x8(ta + N1, yi);
+        } else {
+            tc::ld_x4(ta, yr);
+            tc::ld_x4(ta + N1, yi);
         }
         tc::wait_ld();
         const int o_re = c * 16 + (n2 >> 2) * 128 + (n2 & 3) * 4;
         const int o_im = o_re + (N2 / 4) * 128;
 #pragma unroll
-        for (int i = 0; i < KH; ++i) {
-            const int k1 = h * KH + i;
-            const V w = twl[(n2 * k1) % N];
+        for (int i = 0; i < KQ; ++i) {
+            const int k1 = part * KQ + i;
+            const V w = twl[(n2 * k1) & (N - 1)];
             const float a = yr[i] * w.x - yi[i] * w.y, b = yr[i] * w.y + yi[i] * w.x;
             float rh, rl, ih, il;
             tc::split_tf32(a, rh, rl);
@@ -278,46 +301,50 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     };
     // P2: D3 -> output tile -> rows of the destination
     auto output = [&](V *dst, int out_cols) {
-        const int q = warp & 3, h = warp >> 2;
+        const int q = warp & 3;
         const int c = lane & 7;
-        if constexpr (C::MT3 == 2) {   // warp half h reads M tile h, every k2
-            const int k1 = (lane >> 3) + 4 * q + 16 * h;
-            float xr[16], xi[16];
-            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + h * C::K3;
-            tc::ld_x16(ta, xr);
-            tc::ld_x16(ta + N2, xi);
-            tc::wait_ld();
-#pragma unroll
-            for (int k2 = 0; k2 < 16; ++k2) outt[(k1 + N1 * k2) * C::LDO + c] = V{xr[k2], xi[k2]};
-        } else {   // one M tile: warp half h reads k2 in [8 h, 8 h + 8)
-            const int k1 = (lane >> 3) + 4 * q;
+        if constexpr (C::MT3 == 2) {   // warps of M tile t = (warp / 4) % 2 read k2 in [8 kh, 8 kh + 8)
+            const int t = (warp >> 2) & 1, kh = warp >> 3;
+            const int k1 = (lane >> 3) + 4 * q + 16 * t;
             float xr[8], xi[8];
-            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + 8 * h;
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + t * C::K3 + 8 * kh;
             tc::ld_x8(ta, xr);
             tc::ld_x8(ta + N2, xi);
             tc::wait_ld();
 #pragma unroll
-            for (int i = 0; i < 8; ++i) outt[(k1 + N1 * (8 * h + i)) * C::LDO + c] = V{xr[i], xi[i]};
+            for (int i = 0; i < 8; ++i) outt[(k1 + N1 * (8 * kh + i)) * C::LDO + c] = V{xr[i], xi[i]};
+        } else {   // one M tile: warps read k2 in [4 part, 4 part + 4)
+            const int part = warp >> 2;
+            const int k1 = (lane >> 3) + 4 * q;
+            float xr[4], xi[4];
+            const uint32_t ta = tmem + ((uint32_t)(32 * q) << 16) + C::D3_COL + 4 * part;
+            tc::ld_x4(ta, xr);
+            tc::ld_x4(ta + N2, xi);
+            tc::wait_ld();
+#pragma unroll
+            for (int i = 0; i < 4; ++i) outt[(k1 + N1 * (4 * part + i)) * C::LDO + c] = V{xr[i], xi[i]};
         }
         tc::fence_before_sync();
         __syncthreads();   // output tile complete; D3 read
-        const int nrow = sp.row_out.count();
-        const int drow = (int)sp.d_row;   // row pitch of the destination (< 2^31 elements per tile)
         const int cc = tid & 7;
-        if (cc < out_cols)
-            for (int rc = tid >> 3; rc < nrow; rc += C::NT / 8) {
-                const int row = sp.row_out.expand(rc);
-                const int r = sp.row_out_compact ? rc : row;
-                dst[r * drow + cc] = outt[row * C::LDO + cc];
+        if (cc < out_cols) {
+#pragma unroll 4
+            for (int k = tid >> 3; k < N; k += C::NT / 8) {
+                const int o = orow[k];
+                if (o >= 0) dst[o + cc] = outt[k * C::LDO + cc];
             }
+        }
         __syncthreads();   // A3's space free again
     };
+    // one thread polls (bounded); the block learns the outcome at the barrier
     auto wait_bar = [&](int b, unsigned parity) -> bool {
-        const bool ok = mbar_wait_bounded(&bar[b], parity, wc.limit);
+        bool ok = true;
+        if (tid == 0) ok = mbar_wait_bounded(&bar[b], parity, wc.limit);
         return !__syncthreads_or(!ok);
     };
 
     // ---- the pipeline over units (tile, output)
+    bool failed = false;
     unsigned unit = 0;
     bool pend1 = false, pend3 = false;   // step 1 of `unit` / step 3 of `unit - 1` issued and not yet awaited
     V *prev_dst = nullptr;
@@ -327,15 +354,17 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         int fi, oc, o, c0;
         decode(item, fi, oc, o, c0);
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
-        if (sp.mask) {   // rows kept by the dealias mask in column `warp`: |row index| <= dmax
-            const double kc = wavenum(c0 + warp, sp.n_col, sp.dk_col);
-            int cnt = 0;
-            for (int d0 = 0; d0 <= N / 2; d0 += 32) {
-                const int d = d0 + lane;
-                const bool ok = d <= N / 2 && !(ksq3(sp.dk_row * (double)d, k_out, kc) > sp.kmax2);
-                cnt += __popc(__ballot_sync(0xffffffffu, ok));
+        if (sp.mask) {   // rows kept by the dealias mask in column `warp` (< NB): |row index| <= dmax
+            if (warp < NB) {
+                const double kc = wavenum(c0 + warp, sp.n_col, sp.dk_col);
+                int cnt = 0;
+                for (int d0 = 0; d0 <= N / 2; d0 += 32) {
+                    const int d = d0 + lane;
+                    const bool ok = d <= N / 2 && !(ksq3(sp.dk_row * (double)d, k_out, kc) > sp.kmax2);
+                    cnt += __popc(__ballot_sync(0xffffffffu, ok));
+                }
+                if (lane == 0) dmax_s[warp] = cnt - 1;
             }
-            if (lane == 0) dmax_s[warp] = cnt - 1;
             __syncthreads();
         }
         const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
@@ -380,9 +409,11 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         }
     }
     if (failed) {   // let the MMAs in flight finish (bounded) before the TMEM is freed
-        if (tid == 0 && err) atomicOr(err, 2u);
-        if (pend3) mbar_wait_bounded(&bar[1], (unit - 1) & 1u, wc.limit);
-        if (pend1) mbar_wait_bounded(&bar[0], unit & 1u, wc.limit);
+        if (tid == 0) {
+            if (err) atomicOr(err, 2u);
+            if (pend3) mbar_wait_bounded(&bar[1], (unit - 1) & 1u, wc.limit);
+            if (pend1) mbar_wait_bounded(&bar[0], unit & 1u, wc.limit);
+        }
     }
     tc::fence_before_sync();
     __syncthreads();

@@ -88,13 +88,26 @@ __device__ __forceinline__ void ld_x8(uint32_t taddr, float *v) {
 }
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// x = hi + lo with hi = x rounded to TF32 (round to nearest, ties away) and lo
-// the exact remainder; the MMA reads lo's leading 19 bits
+__device__ __forceinline__ void ld_x4(uint32_t taddr, float *v) {
+    uint32_t r[4];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr)
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// TF32 rounding of an FP32 value (10 fraction bits, round half away from
+// zero: add half a unit of the 13 dropped bits to the magnitude, then clear them)
+__device__ __forceinline__ float round_tf32(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+// x = hi + lo + (|x| 2^-22 at most): hi = x rounded to TF32, lo = the exact
+// remainder x - hi rounded to TF32 (the MMA would otherwise truncate it)
 __device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
-    uint32_t h;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-    hi = __uint_as_float(h);
-    lo = x - hi;
+    hi = round_tf32(x);
+    lo = round_tf32(x - hi);
 }
 
 }  // namespace tc
