@@ -2,10 +2,13 @@
 // gnss_b200.h.
 //
 // Ensemble: many independent jets (uneven grids, Reynolds and Schmidt numbers)
-// stepped together.  Members are spread over a few non-blocking streams; the
-// steps of all members are captured once into one CUDA graph (one branch per
-// stream, members of a branch one after another on a shared scratch buffer)
-// and replayed, so a block of steps of the whole ensemble is one launch.
+// stepped together.  Members of one geometry (grid, precision, scalars, the
+// CN/AB2 scheme, drift coefficient) form groups of up to GNSS_BATCH_MAX whose
+// step is one batched launch per stage (gnss_step_batch: their state,
+// history and scratch lie at fixed strides in one buffer per group).  Groups
+// are spread over a few non-blocking streams; the steps of all groups are
+// captured once into one CUDA graph (one branch per stream) and replayed, so
+// a block of steps of the whole ensemble is one launch.
 //
 // Server: continuous batching.  Submitted requests wait in arrival order; a
 // scheduler thread admits them as soon as an active slot and enough of the
@@ -27,6 +30,7 @@
 #include <vector>
 
 #include "gnss_b200.h"
+#include "internal.h"
 
 namespace {
 
@@ -46,11 +50,30 @@ gnss_fields fields_at(void *base, size_t fb, int nf) {
 struct Member {
     gnss_config cfg{};
     gnss_ctx *ctx = nullptr;
-    void *buf = nullptr;   // state (nf fields) then history (nf fields)
+    void *buf = nullptr;   // state (nf fields) then history (nf fields), in its group's buffer
     gnss_fields state{}, hist{};
+    int group = 0;
+};
+
+// Members of one geometry stepped by one batched launch per stage (or, for a
+// scheme the batches do not serve, one after another).
+struct Group {
+    std::vector<int> members;
+    void *buf = nullptr;       // the members' state and history slots
+    void *scratch = nullptr;   // the members' scratch slices
+    size_t slot = 0;           // bytes per member slot (state + history), a multiple of 256
+    size_t slice = 0;          // bytes per member scratch slice, a multiple of 256
+    bool batched = false;
     int branch = 0;
+    double points = 0.0;
     long long launches_per_step = 0;
 };
+
+bool same_geometry(const gnss_config &a, const gnss_config &b) {
+    return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.precision == b.precision &&
+           a.n_scalars == b.n_scalars && a.scheme == b.scheme && a.alpha == b.alpha && a.lx == b.lx &&
+           a.ly == b.ly && a.lz == b.lz && a.alias_filter == b.alias_filter;
+}
 
 }  // namespace
 
@@ -58,10 +81,10 @@ struct Member {
 struct gnss_ensemble {
     int device = 0;
     std::vector<Member> m;
+    std::vector<Group> groups;
     int nbranch = 1;
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> ev_join;
-    std::vector<void *> branch_scratch;
     cudaEvent_t ev_fork = nullptr;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -74,11 +97,12 @@ static void ensemble_free(gnss_ensemble *e) {
     cudaSetDevice(e->device);
     cudaDeviceSynchronize();
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
-    for (Member &mb : e->m) {
+    for (Member &mb : e->m)
         if (mb.ctx) gnss_destroy(mb.ctx);
-        if (mb.buf) cudaFree(mb.buf);
+    for (Group &g : e->groups) {
+        if (g.buf) cudaFree(g.buf);
+        if (g.scratch) cudaFree(g.scratch);
     }
-    for (void *p : e->branch_scratch) if (p) cudaFree(p);
     for (cudaStream_t s : e->streams) if (s) cudaStreamDestroy(s);
     for (cudaEvent_t ev : e->ev_join) if (ev) cudaEventDestroy(ev);
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
@@ -95,59 +119,83 @@ gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n, int nbranch, gn
     if (cudaSetDevice(dev) != cudaSuccess) return GNSS_ERR_CUDA;
     gnss_ensemble *e = new gnss_ensemble;
     e->device = dev;
-    e->nbranch = std::min(nbranch, n);
     e->m.resize(n);
     gnss_status st = GNSS_OK;
     for (int i = 0; i < n && st == GNSS_OK; ++i) {
+        e->m[i].cfg = cfgs[i];
+        st = gnss_create(&cfgs[i], &e->m[i].ctx);
+    }
+    // groups: members of one geometry, at most GNSS_BATCH_MAX each; batched when the scheme is CN/AB2
+    for (int i = 0; i < n && st == GNSS_OK; ++i) {
         Member &mb = e->m[i];
-        mb.cfg = cfgs[i];
-        st = gnss_create(&cfgs[i], &mb.ctx);
-        if (st) break;
-        const size_t fb = field_bytes_of(mb.cfg);
-        const int nf = nfields_of(mb.cfg);
-        if (cudaMalloc(&mb.buf, 2 * nf * fb) != cudaSuccess || cudaMemset(mb.buf, 0, 2 * nf * fb) != cudaSuccess) {
+        int gi = -1;
+        for (int j = 0; j < (int)e->groups.size(); ++j) {
+            const Group &g = e->groups[j];
+            if ((int)g.members.size() < GNSS_BATCH_MAX && same_geometry(e->m[g.members[0]].cfg, mb.cfg)) {
+                gi = j;
+                break;
+            }
+        }
+        if (gi < 0) {
+            gi = (int)e->groups.size();
+            e->groups.emplace_back();
+            e->groups[gi].batched = mb.cfg.scheme == GNSS_SCHEME_CNAB2;
+        }
+        e->groups[gi].members.push_back(i);
+        mb.group = gi;
+    }
+    // per group: one buffer of member slots (state + history) and one of scratch slices
+    for (size_t gi = 0; gi < e->groups.size() && st == GNSS_OK; ++gi) {
+        Group &g = e->groups[gi];
+        const gnss_config &c0 = e->m[g.members[0]].cfg;
+        const size_t fb = field_bytes_of(c0);
+        const int nf = nfields_of(c0);
+        const size_t k = g.members.size();
+        g.slot = round256(2 * (size_t)nf * fb);
+        g.slice = round256(std::max(gnss_scratch_bytes(e->m[g.members[0]].ctx),
+                                    gnss_batch_scratch_bytes(e->m[g.members[0]].ctx)));
+        g.points = (double)k * c0.nx * c0.ny * c0.nz;
+        if (cudaMalloc(&g.buf, k * g.slot) != cudaSuccess || cudaMemset(g.buf, 0, k * g.slot) != cudaSuccess ||
+            cudaMalloc(&g.scratch, k * g.slice) != cudaSuccess) {
             cudaGetLastError();
-            mb.buf = nullptr;
             st = GNSS_ERR_NOMEM;
             break;
         }
-        mb.state = fields_at(mb.buf, fb, nf);
-        mb.hist = fields_at(static_cast<char *>(mb.buf) + nf * fb, fb, nf);
+        for (size_t j = 0; j < k && st == GNSS_OK; ++j) {
+            Member &mb = e->m[g.members[j]];
+            mb.buf = static_cast<char *>(g.buf) + j * g.slot;
+            mb.state = fields_at(mb.buf, fb, nf);
+            mb.hist = fields_at(static_cast<char *>(mb.buf) + nf * fb, fb, nf);
+            st = gnss_attach_scratch(mb.ctx, static_cast<char *>(g.scratch) + j * g.slice, g.slice);
+        }
     }
     if (st) {
+        cudaGetLastError();
         ensemble_free(e);
         return st;
     }
-    // longest processing time first: each member (by points) to the least-loaded branch
-    std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
-    auto pts = [&](int i) { return (double)e->m[i].cfg.nx * e->m[i].cfg.ny * e->m[i].cfg.nz; };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pts(a) > pts(b); });
+    // longest processing time first: each group (by points) to the least-loaded branch
+    e->nbranch = std::min(nbranch, (int)e->groups.size());
+    std::vector<int> order(e->groups.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return e->groups[a].points > e->groups[b].points; });
     std::vector<double> load(e->nbranch, 0.0);
-    std::vector<size_t> need(e->nbranch, 0);
-    for (int i : order) {
+    for (int gi : order) {
         const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        e->m[i].branch = b;
-        load[b] += pts(i);
-        need[b] = std::max(need[b], round256(gnss_scratch_bytes(e->m[i].ctx)));
+        e->groups[gi].branch = b;
+        load[b] += e->groups[gi].points;
     }
     e->streams.assign(e->nbranch, nullptr);
     e->ev_join.assign(e->nbranch, nullptr);
-    e->branch_scratch.assign(e->nbranch, nullptr);
     for (int b = 0; b < e->nbranch && st == GNSS_OK; ++b) {
         if (cudaStreamCreateWithFlags(&e->streams[b], cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&e->ev_join[b], cudaEventDisableTiming) != cudaSuccess)
             st = GNSS_ERR_CUDA;
-        else if (need[b] && cudaMalloc(&e->branch_scratch[b], need[b]) != cudaSuccess)
-            st = GNSS_ERR_NOMEM;
     }
     if (!st && (cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
                 cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking) != cudaSuccess))
         st = GNSS_ERR_CUDA;
-    for (int i = 0; i < n && !st; ++i) {
-        const int b = e->m[i].branch;
-        st = gnss_attach_scratch(e->m[i].ctx, e->branch_scratch[b], need[b]);
-    }
     if (st) {
         cudaGetLastError();
         ensemble_free(e);
@@ -206,23 +254,48 @@ gnss_status gnss_ensemble_download(gnss_ensemble *e, int i, void *host_state, vo
 long long gnss_ensemble_launches_per_step(const gnss_ensemble *e) {
     if (!e) return 0;
     long long s = 0;
-    for (const Member &mb : e->m) s += mb.launches_per_step;
+    for (const Group &g : e->groups) s += g.launches_per_step;
     return s;
 }
 
-// Every member's steps in branch order on the branch streams, forked from and
-// joined back into stream `s`.
+// Group g's step as the ensemble runs it (one batched step, or the members'
+// own steps), on the group's branch stream.
+static gnss_status group_step(gnss_ensemble *e, Group &g, int euler, cudaStream_t bs) {
+    gnss_ctx *ctxs[GNSS_BATCH_MAX];
+    for (size_t j = 0; j < g.members.size(); ++j) ctxs[j] = e->m[g.members[j]].ctx;
+    const Member &m0 = e->m[g.members[0]];
+    if (g.batched)
+        return gnss_step_batch(ctxs, (int)g.members.size(), &m0.state, &m0.hist, g.slot, g.scratch, g.slice, euler,
+                               bs);
+    for (int i : g.members) {
+        Member &mb = e->m[i];
+        gnss_status st = gnss_step(mb.ctx, &mb.state, &mb.hist, euler, bs);
+        if (st) return st;
+    }
+    return GNSS_OK;
+}
+
+// Tensor-core passes exist for FP32 x / y lengths 256 and 512.
+static bool has_tensor_pass(const gnss_config &c) {
+    return c.precision == GNSS_FP32 && (c.nx == 256 || c.nx == 512 || c.ny == 256 || c.ny == 512);
+}
+
+// Every group's steps in branch order on the branch streams, forked from and
+// joined back into stream `s`: one batched step per group, or the members'
+// own steps one after another.
 static gnss_status ensemble_issue(gnss_ensemble *e, int n_steps, int euler_first, cudaStream_t s) {
     if (cudaEventRecord(e->ev_fork, s) != cudaSuccess) return GNSS_ERR_CUDA;
     for (int b = 0; b < e->nbranch; ++b)
         if (cudaStreamWaitEvent(e->streams[b], e->ev_fork, 0) != cudaSuccess) return GNSS_ERR_CUDA;
-    for (Member &mb : e->m) {
-        const cudaStream_t bs = e->streams[mb.branch];
+    for (Group &g : e->groups) {
+        const cudaStream_t bs = e->streams[g.branch];
         for (int k = 0; k < n_steps; ++k) {
-            const long long l0 = gnss_launch_count(mb.ctx);
-            gnss_status st = gnss_step(mb.ctx, &mb.state, &mb.hist, (euler_first && k == 0) ? 1 : 0, bs);
+            long long l0 = 0, l1 = 0;
+            for (int i : g.members) l0 += gnss_launch_count(e->m[i].ctx);
+            gnss_status st = group_step(e, g, (euler_first && k == 0) ? 1 : 0, bs);
             if (st) return st;
-            mb.launches_per_step = gnss_launch_count(mb.ctx) - l0;
+            for (int i : g.members) l1 += gnss_launch_count(e->m[i].ctx);
+            g.launches_per_step = l1 - l0;
         }
     }
     for (int b = 0; b < e->nbranch; ++b) {
@@ -276,54 +349,52 @@ gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream) {
 gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     if (!e || steps < 1) return GNSS_ERR_INVALID;
     if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
-    using Key = std::tuple<int, int, int, int, int, int, bool>;
-    std::map<Key, int> best;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     gnss_status st = GNSS_OK;
     const int zvariants[3] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED, GNSS_VARIANT_WARPSPEC};
-    const int pvariants[2] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED};
-    auto key_of = [](const gnss_config &c) {
-        return Key{c.nx, c.ny, c.nz, c.precision, c.n_scalars, c.scheme, c.alpha != 0.0};
-    };
-    for (Member &mb : e->m) {
-        const Key k = key_of(mb.cfg);
-        if (best.count(k)) continue;
-        const cudaStream_t bs = e->streams[mb.branch];
+    const int pvariants[3] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED, GNSS_VARIANT_TENSOR};
+    std::vector<int> best(e->groups.size(), GNSS_VARIANT_AUTO);
+    for (size_t gi = 0; gi < e->groups.size() && !st; ++gi) {
+        Group &g = e->groups[gi];
+        const Member &m0 = e->m[g.members[0]];
+        const cudaStream_t bs = e->streams[g.branch];
         float tbest = 0.f;
-        int vbest = 0;
-        for (int combo = 0; combo < 6; ++combo) {
+        int vbest = -1;
+        for (int combo = 0; combo < 9; ++combo) {
             const int zv = zvariants[combo % 3], pv = pvariants[combo / 3];
+            if (pv == GNSS_VARIANT_TENSOR && !has_tensor_pass(m0.cfg)) continue;
             const int v = zv + 4 * pv;   // z variant + 4 * pass variant
-            if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, zv)) ||
-                (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, pv)))
-                break;
+            for (int i : g.members)
+                if ((st = gnss_set_option(e->m[i].ctx, GNSS_OPT_ZVARIANT, zv)) ||
+                    (st = gnss_set_option(e->m[i].ctx, GNSS_OPT_PVARIANT, pv)))
+                    break;
+            if (st) break;
             int zk = 0;
-            if (zv == GNSS_VARIANT_WARPSPEC && (gnss_get_option(mb.ctx, GNSS_OPT_ZKERNEL, &zk) || zk != zv))
+            if (zv == GNSS_VARIANT_WARPSPEC && (gnss_get_option(m0.ctx, GNSS_OPT_ZKERNEL, &zk) || zk != zv))
                 continue;   // no warp-specialised kernel here: the same kernels as the register choice
-            if ((st = gnss_step(mb.ctx, &mb.state, &mb.hist, 1, bs))) break;   // warm-up
+            if ((st = group_step(e, g, 1, bs))) break;   // warm-up
             cudaEventRecord(t0, bs);
-            for (int i = 0; i < steps && !st; ++i) st = gnss_step(mb.ctx, &mb.state, &mb.hist, 0, bs);
+            for (int i = 0; i < steps && !st; ++i) st = group_step(e, g, 0, bs);
             cudaEventRecord(t1, bs);
             if (st) break;
             cudaEventSynchronize(t1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, t0, t1);
-            if (combo == 0 || ms < tbest) {
+            if (vbest < 0 || ms < tbest) {
                 tbest = ms;
                 vbest = v;
             }
         }
-        if (st) break;
-        best[k] = vbest;
+        if (!st) best[gi] = vbest;
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (st) return st;
     for (size_t i = 0; i < e->m.size(); ++i) {
         Member &mb = e->m[i];
-        const int v = best[key_of(mb.cfg)];
+        const int v = best[mb.group];
         if ((st = gnss_set_option(mb.ctx, GNSS_OPT_ZVARIANT, v & 3)) ||
             (st = gnss_set_option(mb.ctx, GNSS_OPT_PVARIANT, v >> 2)))
             return st;

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "gnss_b200.h"
+#include "internal.h"
 #include "kernels.cuh"
 #include "zreg.cuh"
 #include "passreg.cuh"
@@ -207,7 +208,7 @@ template <typename T, int N> struct Launch {
                 PassSpec s8 = sp;
                 const int cols = sp.ncols > sp.out_ncols ? sp.ncols : sp.out_ncols;
                 s8.ncolblk = (cols + C::NB - 1) / C::NB;
-                const long long nitems = (long long)s8.nin * s8.outer.count() * s8.ncolblk;
+                const long long nitems = (long long)s8.nmem * s8.nin * s8.outer.count() * s8.ncolblk;
                 long long grid = (long long)ps * nsm;
                 if (grid > nitems) grid = nitems;
                 kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(reinterpret_cast<const PassPtrs<float> &>(P), s8,
@@ -233,7 +234,7 @@ template <typename T, int N> struct Launch {
                     ps = blocks_per_sm(kern, C::NT, C::SMEM);
                     per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
                 }
-                const long long nitems = (long long)sp.nin * sp.outer.count() * sp.ncolblk;
+                const long long nitems = (long long)sp.nmem * sp.nin * sp.outer.count() * sp.ncolblk;
                 long long grid = (long long)ps * nsm;
                 if (grid > nitems) grid = nitems;
                 kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(P, sp, reinterpret_cast<const V2<T> *>(tw));
@@ -250,7 +251,7 @@ template <typename T, int N> struct Launch {
             ps = blocks_per_sm(kern, C::NT, C::SMEM);
             per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
         }
-        const long long nitems = (long long)sp.nin * sp.outer.count() * sp.ncolblk;
+        const long long nitems = (long long)sp.nmem * sp.nin * sp.outer.count() * sp.ncolblk;
         long long grid = (long long)ps * nsm;
         if (grid > nitems) grid = nitems;
         kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(P, sp, reinterpret_cast<const V2<T> *>(tw));
@@ -271,7 +272,7 @@ template <typename T, int N> struct Launch {
     template <int NPH, int NRAW, bool PP>
     static cudaError_t zphys_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
                                int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
-                               cudaStream_t s) {
+                               cudaStream_t s, int nmem, long long ms) {
         using C = ZPCfg<T, N>;
         const int pipe_b = C::pipe_bytes(NPH, NRAW, ncp, PP);
         const int pipe = pipe_b <= C::SMEM_MAX ? 1 : 0;
@@ -280,29 +281,30 @@ template <typename T, int N> struct Launch {
         cudaError_t e = prep_smem(kern, smem);
         if (e != cudaSuccess) return e;
         int per_sm = blocks_per_sm(kern, NPH * 32, smem);
-        const long long npairs = nlines / 2;
+        const long long mpairs = nlines / 2, npairs = mpairs * nmem;
         long long grid = (long long)per_sm * nsm;
         if (grid > npairs) grid = npairs;
         kern<<<(unsigned)grid, NPH * 32, smem, s>>>(f, zr, nout, npairs, ncp, nkz, pipe, scale, alpha, dkz,
-                                                     reinterpret_cast<const V2<T> *>(tw), err);
+                                                     reinterpret_cast<const V2<T> *>(tw), err, mpairs, ms);
         return cudaGetLastError();
     }
     // ping-pong banks when they fit next to the staging area, else in place
     template <int NPH, int NRAW>
     static cudaError_t zphys_n(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
                                int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
-                               cudaStream_t s) {
+                               cudaStream_t s, int nmem, long long ms) {
         using C = ZPCfg<T, N>;
         if (C::pipe_bytes(NPH, NRAW, ncp, true) <= C::SMEM_MAX)
-            return zphys_k<NPH, NRAW, true>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
-        return zphys_k<NPH, NRAW, false>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            return zphys_k<NPH, NRAW, true>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem,
+                                            ms);
+        return zphys_k<NPH, NRAW, false>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
     }
     // register-resident line transforms (N = 64 .. 512, zr_size) when their shared memory fits
     // diag != nullptr: the instantiation that also writes per-block vorticity sums there
     template <int NPH, int NRAW>
     static cudaError_t zreg_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
                               T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s,
-                              double *diag = nullptr) {
+                              double *diag, int nmem, long long ms) {
         if constexpr (zr_size(N)) {
             const int smem = ZRCfg<T, N>::smem_bytes(NPH, NRAW, ncp);
             if (smem > ZPCfg<T, N>::SMEM_MAX) return cudaErrorNotSupported;
@@ -310,22 +312,23 @@ template <typename T, int N> struct Launch {
             cudaError_t e = prep_smem(kern, smem);
             if (e != cudaSuccess) return e;
             const int per_sm = blocks_per_sm(kern, NPH * 32, smem);
-            const long long npairs = nlines / 2;
+            const long long mpairs = nlines / 2, npairs = mpairs * nmem;
             long long grid = (long long)per_sm * nsm;
             if (grid > npairs) grid = npairs;
             if (diag && grid > STAT_BLOCKS) grid = STAT_BLOCKS;   // one row of sums per block
             kern<<<(unsigned)grid, NPH * 32, smem, s>>>(f, zr, nout, npairs, ncp, nkz, scale, alpha, dkz,
-                                                         reinterpret_cast<const V2<T> *>(tw), err, diag);
+                                                         reinterpret_cast<const V2<T> *>(tw), err, diag, mpairs, ms);
             return cudaGetLastError();
         } else {
             (void)f; (void)zr; (void)nout; (void)nlines; (void)ncp; (void)nkz; (void)scale; (void)alpha; (void)dkz;
-            (void)tw; (void)err; (void)nsm; (void)s; (void)diag;
+            (void)tw; (void)err; (void)nsm; (void)s; (void)diag; (void)nmem; (void)ms;
             return cudaErrorNotSupported;
         }
     }
     // warp-specialised register z kernel (FP32, 9 quantities, 4 products)
     static cudaError_t zws_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
-                             T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s) {
+                             T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s,
+                             int nmem, long long ms) {
         if constexpr ((N == 256 || N == 512) && sizeof(T) == 4) {
             const int smem = ZRCfg<T, N>::smem_bytes_ws(ZWS_NPH, ZWS_NOUT, 10, ncp);
             auto kern = k_zws<T, N, ZWS_NPH, 10>;
@@ -333,15 +336,15 @@ template <typename T, int N> struct Launch {
             if (e != cudaSuccess) return e;
             const int nt = (ZWS_NPH + ZWS_NOUT) * 32;
             const int per_sm = blocks_per_sm(kern, nt, smem);
-            const long long npairs = nlines / 2;
+            const long long mpairs = nlines / 2, npairs = mpairs * nmem;
             long long grid = (long long)per_sm * nsm;
             if (grid > npairs) grid = npairs;
             kern<<<(unsigned)grid, nt, smem, s>>>(f, zr, nout, npairs, ncp, nkz, scale, alpha, dkz,
-                                                   reinterpret_cast<const V2<T> *>(tw), err);
+                                                   reinterpret_cast<const V2<T> *>(tw), err, mpairs, ms);
             return cudaGetLastError();
         } else {
             (void)f; (void)zr; (void)nout; (void)nlines; (void)ncp; (void)nkz; (void)scale; (void)alpha; (void)dkz;
-            (void)tw; (void)err; (void)nsm; (void)s;
+            (void)tw; (void)err; (void)nsm; (void)s; (void)nmem; (void)ms;
             return cudaErrorNotSupported;
         }
     }
@@ -369,35 +372,39 @@ template <typename T, int N> struct Launch {
     // not exist)
     static cudaError_t zphys(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                              long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
-                             unsigned *err, int nsm, cudaStream_t s, int zvariant, double *diag = nullptr) {
+                             unsigned *err, int nsm, cudaStream_t s, int zvariant, double *diag = nullptr,
+                             int nmem = 1, long long ms = 0) {
         if (diag) {
             if (!zreg_fits(nph, nraw, ncp)) return cudaErrorNotSupported;
             if (nph == 9 && nraw == 10)
-                return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag);
+                return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag, 1, 0);
             if (nph == 12 && nraw == 13)
-                return zreg_k<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag);
+                return zreg_k<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag, 1, 0);
             if (nph == 14 && nraw == 14)
-                return zreg_k<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag);
+                return zreg_k<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, diag, 1, 0);
             return cudaErrorInvalidValue;
         }
         const int kern = zkernel(zvariant, nph, nraw, nout, ncp);
         if (kern == GNSS_VARIANT_WARPSPEC)
-            return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
         if (kern == GNSS_VARIANT_REGISTER) {
             if (nph == 9 && nraw == 10)
-                return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+                return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nullptr, nmem,
+                                     ms);
             if (nph == 12 && nraw == 13)
-                return zreg_k<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+                return zreg_k<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nullptr, nmem,
+                                      ms);
             if (nph == 14 && nraw == 14)
-                return zreg_k<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+                return zreg_k<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nullptr, nmem,
+                                      ms);
             return cudaErrorInvalidValue;
         }
         if (nph == 9 && nraw == 10)
-            return zphys_n<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            return zphys_n<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
         if (nph == 12 && nraw == 13)
-            return zphys_n<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            return zphys_n<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
         if (nph == 14 && nraw == 14)
-            return zphys_n<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s);
+            return zphys_n<14, 14>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
         return cudaErrorInvalidValue;
     }
 };
@@ -434,9 +441,10 @@ static cudaError_t launch_zpass(int n, int dir, const FieldSet<T> &f, int nfield
 template <typename T>
 static cudaError_t launch_zphys(int n, const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout,
                                 long long nlines, int ncp, int nkz, T scale, T alpha, double dkz, const void *tw,
-                                unsigned *err, int nsm, cudaStream_t s, int zvariant, double *diag = nullptr) {
+                                unsigned *err, int nsm, cudaStream_t s, int zvariant, double *diag = nullptr,
+                                int nmem = 1, long long ms = 0) {
     GNSS_SIZE_SWITCH(n, return (Launch<T, NN_>::zphys(f, zr, nph, nraw, nout, nlines, ncp, nkz, scale, alpha, dkz, tw,
-                                                      err, nsm, s, zvariant, diag)));
+                                                      err, nsm, s, zvariant, diag, nmem, ms)));
 }
 
 template <typename T> static int pass_nb(int n) {
@@ -499,6 +507,7 @@ static KeepMap keep_all(int n) { return KeepMap{n, -1}; }
 template <typename T> static PassSpec base_spec(const gnss_ctx *c, int nrow_fft, int nin) {
     const Geom &g = c->g;
     PassSpec p{};
+    p.nmem = 1;
     const int nb = pass_nb<T>(nrow_fft);
     p.ncols = g.nz2;
     p.out_ncols = g.nz2;
@@ -646,15 +655,28 @@ template <typename T> static gnss_status inverse_t(gnss_ctx *c, void *f, cudaStr
 //   4 y forward of the products (in place)                                 (Q)
 //   5 x forward of the products into the spectral layout                   (Q -> P)
 //   6 projection, dealias and time update                                  (P, state, hist)
+// A batch: nmem members of one geometry stepped by the same launches (the
+// ensemble's size groups).  Member m's state and history fields lie ms_sh
+// elements after member 0's, its step scratch ms_scr elements after the
+// batch scratch `scratch`; mc holds the members' update coefficients.
+struct Batch {
+    int nmem = 1;
+    long long ms_sh = 0, ms_scr = 0;
+    void *scratch = nullptr;
+    const MemberCoef *mc = nullptr;
+};
+
 template <typename T>
 static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, void *hist_base, const gnss_fields *hist,
                                         const UpdCoef &uc, cudaStream_t s, double *stats_dst = nullptr,
-                                        double *diag = nullptr) {
+                                        double *diag = nullptr, const Batch &bt = Batch{}) {
     const Geom &g = c->g;
     const int np = c->n_xout, nq = c->n_raw, nnl = c->nnl;
-    gnss_status st = ensure_scratch_step(c);
-    if (st) return st;
-    V2<T> *Pb = reinterpret_cast<V2<T> *>(c->scratch);
+    if (!bt.scratch) {
+        gnss_status st = ensure_scratch_step(c);
+        if (st) return st;
+    }
+    V2<T> *Pb = reinterpret_cast<V2<T> *>(bt.scratch ? bt.scratch : c->scratch);
     V2<T> *Qb = Pb + c->p_elems * (size_t)np;
     auto Pf = [&](int q) { return Pb + c->p_elems * (size_t)q; };
     auto Qf = [&](int q) { return Qb + c->q_elems * (size_t)q; };
@@ -682,6 +704,7 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             spx.nvar[i] = c->xvar_n[i];
             for (int v = 0; v < 2; ++v) { spx.vmul[i][v] = c->xvar_mul[i][v]; spx.vout[i][v] = c->xvar_out[i][v]; }
         }
+        spx.nmem = bt.nmem; spx.ms_in = bt.ms_sh; spx.ms_out = bt.ms_scr;
         CK(c, launch_pass<T>(g.nx, +1, P, spx, c->tw[0], c->nsm, s, c->pvariant, c->d_err));
     }
     {
@@ -694,31 +717,48 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
             spy.nvar[i] = c->yvar_n[i];
             for (int v = 0; v < 2; ++v) { spy.vmul[i][v] = c->yvar_mul[i][v]; spy.vout[i][v] = c->yvar_out[i][v]; }
         }
+        spy.nmem = bt.nmem; spy.ms_in = spy.ms_out = bt.ms_scr;
         CK(c, launch_pass<T>(g.ny, +1, P, spy, c->tw[1], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 2);
         CK(c, launch_zphys<T>(g.nz, Q, c->zrec, c->n_phys, nq, nnl, nlines, c->ncp, c->nkz, scale, (T)c->cfg.alpha,
-                              g.dkz, c->tw[2], c->d_err, c->nsm, s, c->zvariant, diag));
+                              g.dkz, c->tw[2], c->d_err, c->nsm, s, c->zvariant, diag, bt.nmem, bt.ms_scr));
     }
     {
         StageTimer t(c, s, 3);
         PassPtrs<T> P{};
         for (int q = 0; q < nnl; ++q) { P.in[q] = Qf(q); P.out[q] = Pf(q); }
-        CK(c, launch_pass<T>(g.ny, -1, P, step_spec<T>(c, Y_FWD_STEP, nnl), c->tw[1], c->nsm, s, c->pvariant, c->d_err));
+        PassSpec sp3 = step_spec<T>(c, Y_FWD_STEP, nnl);
+        sp3.nmem = bt.nmem; sp3.ms_in = sp3.ms_out = bt.ms_scr;
+        CK(c, launch_pass<T>(g.ny, -1, P, sp3, c->tw[1], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 4);
         PassPtrs<T> P{};
         for (int q = 0; q < nnl; ++q) { P.in[q] = Pf(q); P.out[q] = R.p[q]; }
-        CK(c, launch_pass<T>(g.nx, -1, P, step_spec<T>(c, X_FWD_STEP, nnl), c->tw[0], c->nsm, s, c->pvariant, c->d_err));
+        PassSpec sp4 = step_spec<T>(c, X_FWD_STEP, nnl);
+        sp4.nmem = bt.nmem; sp4.ms_in = sp4.ms_out = bt.ms_scr;
+        CK(c, launch_pass<T>(g.nx, -1, P, sp4, c->tw[0], c->nsm, s, c->pvariant, c->d_err));
     }
     {
         StageTimer t(c, s, 5);
         // one warp per kept (ky, kx) row; 8 blocks of 8 warps per SM
-        const long long nrows = (long long)c->ky_keep.count() * c->kx_keep.count();
+        const long long nrows = (long long)c->ky_keep.count() * c->kx_keep.count() * bt.nmem;
         const int full_rows = (uc.scheme == GNSS_SCHEME_CNAB2 && uc.euler) ? 1 : 0;
         long long nblk = std::min<long long>((nrows + 7) / 8, 8LL * c->nsm);
+        if (bt.nmem > 1) {   // a batch (no statistics): per-member coefficients and mean lines
+            if (uc.scheme == GNSS_SCHEME_CNAB2)
+                k_update_batch<T, GNSS_SCHEME_CNAB2><<<(unsigned)nblk, 256, 0, s>>>(
+                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, *bt.mc, bt.nmem, bt.ms_sh,
+                    bt.ms_scr);
+            else
+                k_update_batch<T, GNSS_SCHEME_RK3IF><<<(unsigned)nblk, 256, 0, s>>>(
+                    SF, H, R, g, c->kx_keep, c->ky_keep, c->nkz, c->ncp, uc, full_rows, *bt.mc, bt.nmem, bt.ms_sh,
+                    bt.ms_scr);
+            LAUNCH_CK(c);
+            return GNSS_OK;
+        }
         if (stats_dst) {   // statistics of the new state summed by the update itself (one partial row per block)
             nblk = std::min<long long>(nblk, STAT_BLOCKS);
             if (uc.scheme == GNSS_SCHEME_CNAB2)
@@ -1546,6 +1586,59 @@ static bool state_ok(const gnss_ctx *c, const gnss_fields *st) {
     if (c->cfg.n_scalars > 1 && !st->c) return false;
     return true;
 }
+
+// ============================================================== batches (the ensemble's size groups)
+static_assert(GNSS_BATCH_MAX <= MAXM, "batch size");
+
+size_t gnss_batch_scratch_bytes(const gnss_ctx *c) { return c ? step_scratch_elems(c) * c->elem : 0; }
+
+template <typename T>
+static gnss_status step_batch_t(gnss_ctx *const *cs, int n, const gnss_fields *st0, const gnss_fields *hi0,
+                                long long ms_sh, void *scratch, long long ms_scr, int euler, cudaStream_t s) {
+    gnss_ctx *c = cs[0];
+    UpdCoef uc = base_coef(c);
+    uc.euler = euler ? 1 : 0;
+    MemberCoef mc{};
+    for (int m = 0; m < n; ++m) {
+        const UpdCoef u = base_coef(cs[m]);
+        mc.dt[m] = u.dt;
+        for (int q = 0; q < 5; ++q) {
+            mc.hnum[m][q] = u.hnum[q];
+            mc.nu[m][q] = u.nu[q];
+        }
+        mc.mean[m] = cs[m]->mean64;
+    }
+    Batch bt;
+    bt.nmem = n;
+    bt.ms_sh = ms_sh;
+    bt.ms_scr = ms_scr;
+    bt.scratch = scratch;
+    bt.mc = &mc;
+    return nonlinear_and_update<T>(c, st0, nullptr, hi0, uc, s, nullptr, nullptr, bt);
+}
+
+gnss_status gnss_step_batch(gnss_ctx *const *cs, int n, const gnss_fields *st0, const gnss_fields *hi0,
+                            size_t member_bytes, void *scratch, size_t scratch_bytes, int euler, void *stream) {
+    if (!cs || n < 1 || n > GNSS_BATCH_MAX || !cs[0] || !scratch) return GNSS_ERR_INVALID;
+    gnss_ctx *c = cs[0];
+    const gnss_config &k = c->cfg;
+    if (k.scheme != GNSS_SCHEME_CNAB2) return fail(c, GNSS_ERR_UNSUPPORTED, "batched steps use the CN/AB2 scheme");
+    for (int m = 1; m < n; ++m) {
+        const gnss_config &o = cs[m] ? cs[m]->cfg : k;
+        if (!cs[m] || o.nx != k.nx || o.ny != k.ny || o.nz != k.nz || o.precision != k.precision ||
+            o.n_scalars != k.n_scalars || o.scheme != k.scheme || o.alpha != k.alpha || o.device != k.device ||
+            o.lx != k.lx || o.ly != k.ly || o.lz != k.lz || o.alias_filter != k.alias_filter)
+            return fail(c, GNSS_ERR_INVALID, "member %d of a batch has another geometry", m);
+    }
+    if (!state_ok(c, st0) || !state_ok(c, hi0)) return fail(c, GNSS_ERR_INVALID, "state or history fields missing");
+    if (!al_fields(c, st0) || !al_fields(c, hi0) || member_bytes % c->elem || scratch_bytes % 256 ||
+        reinterpret_cast<uintptr_t>(scratch) % 256 || scratch_bytes < gnss_batch_scratch_bytes(c))
+        return fail(c, GNSS_ERR_INVALID, "misaligned or short batch buffers");
+    CK(c, cudaSetDevice(k.device));
+    const long long ms_sh = (long long)(member_bytes / c->elem), ms_scr = (long long)(scratch_bytes / c->elem);
+    return PREC_CALL(c, step_batch_t, cs, n, st0, hi0, ms_sh, scratch, ms_scr, euler, S(stream));
+}
+
 
 gnss_status gnss_step(gnss_ctx *c, const gnss_fields *state, const gnss_fields *hist, int euler, void *stream) {
     if (!c) return GNSS_ERR_INVALID;

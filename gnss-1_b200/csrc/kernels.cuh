@@ -83,6 +83,8 @@ struct PassSpec {
     signed char nvar[MAXF];    // outputs per input (1 or 2)
     signed char vmul[MAXF][2]; // multiplier of each output
     signed char vout[MAXF][2]; // output field index of each output
+    int nmem;                  // members of a batch (jets of one geometry in one launch), >= 1
+    long long ms_in, ms_out;   // element strides between the members' inputs / outputs
 };
 template <typename T> struct PassPtrs {
     const V2<T> *in[MAXF];
@@ -145,23 +147,26 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
     V *work = reinterpret_cast<V *>(smem_raw) + 2 * TILE;
     const int tid = threadIdx.x;
     const int ntiles = sp.outer.count() * sp.ncolblk;
-    const long long nitems = (long long)sp.nin * ntiles;
+    const int mitems = sp.nin * ntiles;   // items of one member
+    const long long nitems = (long long)sp.nmem * mitems;
     long long item = blockIdx.x;
     if (item >= nitems) return;
-    // oc: compact outer index, o: expanded outer index
-    // work items fit in 32 bits (inputs x outer indices x column blocks): 32-bit divisions
-    auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
+    // mi: member, oc: compact outer index, o: expanded outer index
+    // work items fit in 32 bits (members x inputs x outer indices x column blocks): 32-bit divisions
+    auto decode = [&](long long it, int &mi, int &fi, int &oc, int &o, int &c0) {
         const int i32 = (int)it;
-        fi = i32 / ntiles;
-        const int t = i32 - fi * ntiles;
+        mi = i32 / mitems;
+        const int r = i32 - mi * mitems;
+        fi = r / ntiles;
+        const int t = r - fi * ntiles;
         oc = t / sp.ncolblk;
         o = sp.outer.expand(oc);
         c0 = (t - oc * sp.ncolblk) * NB;
     };
     auto prefetch = [&](long long it, V *dst) {
-        int fi, oc, o, c0;
-        decode(it, fi, oc, o, c0);
-        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        int mi, fi, oc, o, c0;
+        decode(it, mi, fi, oc, o, c0);
+        const V *src = P.in[fi] + mi * sp.ms_in + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
         tile_prefetch<T, NB, NT, TILE>(dst, src, sp, c0, tid);
     };
     prefetch(item, rawb[0]);
@@ -173,11 +178,11 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
         cp_async_commit();
         cp_async_wait<1>();   // this thread's copies of the current tile have landed
         __syncthreads();      // ... and everybody else's
-        int fi, oc, o, c0;
-        decode(item, fi, oc, o, c0);
+        int mi, fi, oc, o, c0;
+        decode(item, mi, fi, oc, o, c0);
         const V *cur = rawb[buf];
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
-        const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const long long dbase = mi * sp.ms_out + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0;
         const int nv = sp.nvar[fi];
         for (int v = 0; v < nv; ++v) {
@@ -345,6 +350,18 @@ k_zpass(FieldSet<T> f, long long nlines, int nz2, T scale, const V2<T> *__restri
 //   3 u . grad s                             (dotKernel_mgpu, solver.cu:342-356)
 //   4 alpha (lap s c + grad c . grad s) + u . grad c   (colloidAdvectionKernel_mgpu, solver.cu:374-388)
 // One warp per input field; one block per line pair.
+//
+// Batches: the line pairs of nmem members of one geometry are numbered
+// member after member (mpairs per member), and a member's fields lie ms
+// elements after the previous member's; pair p of the batch starts at
+// element pair_offset(p) of each field pointer.  The batch holds fewer than
+// 2^31 pairs.
+__device__ __forceinline__ long long pair_offset(long long p, long long mpairs, long long ms, int rawf) {
+    const int pi = (int)p, mp = (int)mpairs;
+    const int mi = pi / mp;
+    return mi * ms + (long long)(pi - mi * mp) * rawf;
+}
+
 template <typename T, int N> struct ZPCfg {
     static constexpr int LEN = padded_len<T>(N);   // padded line in the work area
     // work area: one bank of nph lines, or two banks when the transforms ping-pong
@@ -471,7 +488,7 @@ template <typename T, int N, int NPH, int NRAW, bool PP>
 __global__ void __launch_bounds__(NPH * 32, (PP && sizeof(T) == 4) ? 2 : 1)
 k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
         int ncp, int nkz, int pipe, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw,
-        unsigned *__restrict__ err) {
+        unsigned *__restrict__ err, long long mpairs, long long ms) {
     using V = V2<T>;
     using C = ZPCfg<T, N>;
     constexpr int LEN = C::LEN;
@@ -501,7 +518,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
         if (!withhold)
-            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset(p, mpairs, ms, rawf), raw_bytes, bar);
     };
     if (pipe && threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
@@ -520,8 +537,8 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
             a0 = raw + rc.r[0] * rawf;
             a1 = rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr;
         } else {
-            a0 = f.p[rc.r[0]] + pair * rawf;
-            a1 = rc.r[1] >= 0 ? f.p[rc.r[1]] + pair * rawf : nullptr;
+            a0 = f.p[rc.r[0]] + pair_offset(pair, mpairs, ms, rawf);
+            a1 = rc.r[1] >= 0 ? f.p[rc.r[1]] + pair_offset(pair, mpairs, ms, rawf) : nullptr;
         }
         pack_c2r_combo<T, N>(lane, lineA, rc, a0, a1, ncp, nkz, dkz);
         __syncthreads();   // staging area (or the raw lines in global memory) consumed
@@ -542,7 +559,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
             V *pl = prod + warp * LEN;
             if constexpr (PP) warp_line_fft_pp<T, N, -1>(lane, pl, (prod == bankA ? bankB : bankA) + warp * LEN, tw);
             else warp_line_fft<T, N, -1>(lane, pl, tw);
-            V *d = f.p[warp] + pair * rawf;
+            V *d = f.p[warp] + pair_offset(pair, mpairs, ms, rawf);
             unpack_r2c_pad<T, N>(lane, 32, fres + warp * LEN, d, d + ncp, ncp);
         }
         __syncthreads();   // work area reused by the next pair
@@ -579,6 +596,16 @@ struct UpdCoef {
     int substep;      // IF-RK3: 0, 1, 2 (substep 0 ignores the history input)
 };
 
+// Per-member update coefficients of a batch (jets of one geometry stepped by
+// one launch; Reynolds and Schmidt numbers and time steps may differ).
+constexpr int MAXM = 16;
+struct MemberCoef {
+    double dt[MAXM];
+    double hnum[MAXM][5];   // CN: dt / 2 / num
+    double nu[MAXM][5];     // IF: diffusivity
+    double2 *mean[MAXM];    // FP32 contexts: the member's FP64 mean-profile line (or null)
+};
+
 // One warp per (ky, kx) row of the kept box, lanes along kz.  The arithmetic
 // follows makeRHS / deAlias / timestep / update (solver.cu:461-657) with the
 // divisions by k^2 and by (1 + dt k^2/(2 num)) done once as reciprocals.
@@ -599,31 +626,41 @@ struct UpdCoef {
 // update); otherwise the field's own value is taken, so a state written
 // anew by the caller starts from what it holds.  Both copies are written.
 //
+// With BATCH, the rows of nmem members follow one another (state and hist of
+// member m ms_sh elements after member 0's, nl ms_nl), and member m takes its
+// coefficients and mean line from mc.
+//
 // With STATS, the kernel also sums, over the modes it writes, the spectral
 // statistics of the new state (the six sums of k_stats_partial: the full
 // spectrum through the kz mirror, statistics.cu:1494-1845) and writes one row
 // of STAT_SUMS partials per block to `partial`; for a state that is zero
 // outside the dealiasing sphere (the precondition of the step) they equal the
 // sums over the whole field.
-template <typename T, int SCHEME, bool STATS = false>
-__global__ void __launch_bounds__(256)
-k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
-         const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
-         UpdCoef c, int full_rows, double *__restrict__ partial = nullptr, double2 *__restrict__ mean = nullptr) {
+template <typename T, int SCHEME, bool STATS, bool BATCH>
+__device__ __forceinline__ void k_update_body(const FieldSet<T> &state, const FieldSet<T> &hist, const FieldSet<T> &nl,
+                                              const Geom &g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
+                                              const UpdCoef &c, int full_rows, double *__restrict__ partial,
+                                              double2 *__restrict__ mean0, const MemberCoef *mc, int nmem,
+                                              long long ms_sh, long long ms_nl) {
     using V = V2<T>;
     double acc[STATS ? STAT_SUMS : 1] = {};
     const int nkx = kx_keep.count(), nky = ky_keep.count();
-    const int nrows = nky * nkx;
+    const int mrows = nky * nkx;   // rows of one member
+    const int nrows = mrows * nmem;
     const int lane = threadIdx.x & 31;
     const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
     const bool read_hist = (SCHEME == 0) ? !c.euler : (c.substep > 0);
     const int nf = c.nf;
-    for (int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); row < nrows; row += nwarp) {
+    for (int brow = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); brow < nrows; brow += nwarp) {
+        const int mi = BATCH ? brow / mrows : 0;
+        const int row = BATCH ? brow - mi * mrows : brow;
         const int kyc = row / nkx, kxc = row - kyc * nkx;
         const int kxi = kx_keep.expand(kxc), kyi = ky_keep.expand(kyc);
         const double k1 = wavenum(kxi, g.nx, g.dkx), k2 = wavenum(kyi, g.ny, g.dky);
-        const long long base = ((long long)kyi * g.nx + kxi) * g.nz2;   // state / hist
-        const long long jbase = (long long)row * ncp;                     // nonlinear term
+        const long long base = ((long long)kyi * g.nx + kxi) * g.nz2 + (BATCH ? mi * ms_sh : 0);   // state / hist
+        const long long jbase = (long long)row * ncp + (BATCH ? mi * ms_nl : 0);                    // nonlinear term
+        double2 *const mean = BATCH ? mc->mean[mi] : mean0;
+        const double c_dt = BATCH ? mc->dt[mi] : c.dt;
         for (int k0 = 0; k0 < nkz; k0 += 32) {
             const int kzi = k0 + lane;
             const bool inrow = kzi < nkz;
@@ -700,24 +737,24 @@ k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ Fiel
                 double nr, ni, gr, gi;   // new state and new history
                 if constexpr (SCHEME == 0) {
                     // eulerKernel_mgpu / adamsBashforthKernel_mgpu (solver.cu:547-585)
-                    const double hk = c.hnum[q] * ksq;
+                    const double hk = (BATCH ? mc->hnum[mi][q] : c.hnum[q]) * ksq;
                     const double am = 1.0 - hk;
                     const double ib = 1.0 / (1.0 + hk);
                     if (c.euler) {
-                        nr = (am * fr + c.dt * R[q][0]) * ib;
-                        ni = (am * fi + c.dt * R[q][1]) * ib;
+                        nr = (am * fr + c_dt * R[q][0]) * ib;
+                        ni = (am * fi + c_dt * R[q][1]) * ib;
                     } else {
-                        nr = (am * fr + c.dt * (1.5 * R[q][0] - 0.5 * hr)) * ib;
-                        ni = (am * fi + c.dt * (1.5 * R[q][1] - 0.5 * hi)) * ib;
+                        nr = (am * fr + c_dt * (1.5 * R[q][0] - 0.5 * hr)) * ib;
+                        ni = (am * fi + c_dt * (1.5 * R[q][1] - 0.5 * hi)) * ib;
                     }
                     gr = R[q][0];   // updateKernel_mgpu (solver.cu:618-637)
                     gi = R[q][1];
                 } else {
-                    const double E = exp(-c.nu[q] * ksq * c.alph * c.dt);
-                    nr = E * (fr + c.gam * c.dt * R[q][0] + hr);
-                    ni = E * (fi + c.gam * c.dt * R[q][1] + hi);
-                    gr = c.zet_next * c.dt * E * R[q][0];
-                    gi = c.zet_next * c.dt * E * R[q][1];
+                    const double E = exp(-(BATCH ? mc->nu[mi][q] : c.nu[q]) * ksq * c.alph * c_dt);
+                    nr = E * (fr + c.gam * c_dt * R[q][0] + hr);
+                    ni = E * (fi + c.gam * c_dt * R[q][1] + hi);
+                    gr = c.zet_next * c_dt * E * R[q][0];
+                    gi = c.zet_next * c_dt * E * R[q][1];
                 }
                 state.p[q][idx] = V{(T)nr, (T)ni};
                 if constexpr (STATS) sv[q] = V{(T)nr, (T)ni};
@@ -760,6 +797,24 @@ k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ Fiel
             partial[blockIdx.x * STAT_SUMS + threadIdx.x] = v;
         }
     }
+}
+
+template <typename T, int SCHEME, bool STATS = false, bool BATCH = false>
+__global__ void __launch_bounds__(256)
+k_update(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
+         const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
+         UpdCoef c, int full_rows, double *__restrict__ partial = nullptr, double2 *__restrict__ mean = nullptr) {
+    k_update_body<T, SCHEME, STATS, false>(state, hist, nl, g, kx_keep, ky_keep, nkz, ncp, c, full_rows, partial,
+                                           mean, nullptr, 1, 0, 0);
+}
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(256)
+k_update_batch(const __grid_constant__ FieldSet<T> state, const __grid_constant__ FieldSet<T> hist,
+               const __grid_constant__ FieldSet<T> nl, Geom g, KeepMap kx_keep, KeepMap ky_keep, int nkz, int ncp,
+               UpdCoef c, int full_rows, const __grid_constant__ MemberCoef mc, int nmem, long long ms_sh,
+               long long ms_nl) {
+    k_update_body<T, SCHEME, false, true>(state, hist, nl, g, kx_keep, ky_keep, nkz, ncp, c, full_rows, nullptr,
+                                          nullptr, &mc, nmem, ms_sh, ms_nl);
 }
 
 // ------------------------------------------------------------ statistics

@@ -78,16 +78,19 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     V *tws = outt + TILE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = sp.outer.count() * sp.ncolblk;
-    const long long nitems = (long long)sp.nin * ntiles;
+    const int mitems = sp.nin * ntiles;   // items of one member
+    const long long nitems = (long long)sp.nmem * mitems;
     long long item = blockIdx.x;
     if (item >= nitems) return;
     for (int i = tid; i < C::TWR * 32; i += NT) tws[i] = tw[Z::tw_index(i, true)];
-    // work items fit in 32 bits (inputs x outer indices x column blocks), so they are decoded with 32-bit
-    // divisions
-    auto decode = [&](long long it, int &fi, int &oc, int &o, int &c0) {
+    // work items fit in 32 bits (members x inputs x outer indices x column blocks), so they are decoded with
+    // 32-bit divisions
+    auto decode = [&](long long it, int &mi, int &fi, int &oc, int &o, int &c0) {
         const int i32 = (int)it;
-        fi = i32 / ntiles;
-        const int t = i32 - fi * ntiles;
+        mi = i32 / mitems;
+        const int r = i32 - mi * mitems;
+        fi = r / ntiles;
+        const int t = r - fi * ntiles;
         oc = t / sp.ncolblk;
         o = sp.outer.expand(oc);
         c0 = (t - oc * sp.ncolblk) * NB;
@@ -100,9 +103,9 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     for (int k = 0; k < N / RSTEP; ++k) prow |= (sp.row_in.kept(tid / NB + RSTEP * k) ? 1u : 0u) << k;
     const int s_row = (int)sp.s_row;
     auto prefetch = [&](long long it, V *dst) {
-        int fi, oc, o, c0;
-        decode(it, fi, oc, o, c0);
-        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        int mi, fi, oc, o, c0;
+        decode(it, mi, fi, oc, o, c0);
+        const V *src = P.in[fi] + mi * sp.ms_in + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
         const int b = tid % NB;
         if (c0 + b >= sp.ncols) return;
 #pragma unroll 4
@@ -130,8 +133,8 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
         const long long next = item + gridDim.x;
         if (next < nitems) prefetch(next, tiles + (buf ^ 1) * TILE);
         cp_async_commit();
-        int fi, oc, o, c0;
-        decode(item, fi, oc, o, c0);
+        int mi, fi, oc, o, c0;
+        decode(item, mi, fi, oc, o, c0);
         const V *cur = tiles + buf * TILE;
         const bool col_ok = c0 + b < sp.ncols;
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
@@ -150,7 +153,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             for (int m = 0; m < E; ++m)
                 if (row_dist<N>(lane + 32 * m) > dmax) okm &= ~(1u << m);
         }
-        const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const long long dbase = mi * sp.ms_out + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0;
         const int nv = sp.nvar[fi];
         for (int v = 0; v < nv; ++v) {

@@ -100,7 +100,8 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     unsigned char *sm = smem_raw + (base - raw_addr);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = sp.outer.count() * sp.ncolblk;
-    const int nitems = sp.nin * ntiles;   // < 2^31 (inputs x outer indices x column blocks)
+    const int mitems = sp.nin * ntiles;      // items of one member
+    const int nitems = sp.nmem * mitems;     // < 2^31 (members x inputs x outer indices x column blocks)
     int item = blockIdx.x;
     if (item >= nitems) return;   // uniform for the block
     V *twl = reinterpret_cast<V *>(sm + C::OFF_TW);
@@ -154,9 +155,11 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     const uint32_t tmem = *tslot;
     const WaitCtl wc(err);
 
-    auto decode = [&](int it, int &fi, int &oc, int &o, int &c0) {
-        fi = it / ntiles;
-        const int t = it - fi * ntiles;
+    auto decode = [&](int it, int &mi, int &fi, int &oc, int &o, int &c0) {
+        mi = it / mitems;
+        const int r = it - mi * mitems;
+        fi = r / ntiles;
+        const int t = r - fi * ntiles;
         oc = t / sp.ncolblk;
         o = sp.outer.expand(oc);
         c0 = (t - oc * sp.ncolblk) * NB;
@@ -176,9 +179,9 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
         }
     V raw[NIT][4];
     auto load = [&](int it_item) {
-        int fi, oc, o, c0;
-        decode(it_item, fi, oc, o, c0);
-        const V *src = P.in[fi] + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0 + pc;
+        int mi, fi, oc, o, c0;
+        decode(it_item, mi, fi, oc, o, c0);
+        const V *src = P.in[fi] + mi * sp.ms_in + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0 + pc;
         const bool col_ok = c0 + pc < sp.ncols;
 #pragma unroll
         for (int it = 0; it < NIT; ++it)
@@ -351,8 +354,8 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     int prev_cols = 0;
     load(item);
     while (item < nitems && !failed) {
-        int fi, oc, o, c0;
-        decode(item, fi, oc, o, c0);
+        int mi, fi, oc, o, c0;
+        decode(item, mi, fi, oc, o, c0);
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
         if (sp.mask) {   // rows kept by the dealias mask in column `warp` (< NB): |row index| <= dmax
             if (warp < NB) {
@@ -367,7 +370,7 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
             }
             __syncthreads();
         }
-        const long long dbase = (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const long long dbase = mi * sp.ms_out + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0 < NB ? sp.out_ncols - c0 : NB;
         const int nv = sp.nvar[fi];
         const int next = item + gridDim.x;

@@ -516,8 +516,9 @@ __device__ __forceinline__ void zr_store_r2c(int lane, const V2<T> *x, V2<T> *sc
     __syncwarp();   // scratch reused by the next transform
 }
 
-// Persistent: block b handles line pairs b, b + gridDim.x, ...; warp q forms
-// physical quantity q.  The raw lines of the next pair arrive by
+// Persistent: block b handles line pairs b, b + gridDim.x, ... of all members
+// of a batch (npairs in all, mpairs per member, members ms elements apart);
+// warp q forms physical quantity q.  The raw lines of the next pair arrive by
 // cp.async.bulk (CTA-local, no multicast) while the current pair is
 // processed; a wait that times out sets bit 0 of *err and the block stops.
 // With DIAG the block also writes one row of ZR_VORT_SUMS vorticity sums over
@@ -527,7 +528,7 @@ template <typename T, int N, int NPH, int NRAW, bool DIAG = false>
 __global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? (N <= 192 ? 4 : 3) : (N <= 192 ? 2 : 1))
 k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
        int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err,
-       double *__restrict__ diag = nullptr) {
+       double *__restrict__ diag, long long mpairs, long long ms) {
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
     constexpr int E = Z::E, SCR = Z::SCR;
@@ -560,7 +561,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
         if (!withhold)
-            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset(p, mpairs, ms, rawf), raw_bytes, bar);
     };
     if (threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
@@ -597,7 +598,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
             for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
             __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
-            zr_store_r2c<T, N>(lane, x, scr, f.p[warp] + pair * rawf, ncp);
+            zr_store_r2c<T, N>(lane, x, scr, f.p[warp] + pair_offset(pair, mpairs, ms, rawf), ncp);
         }
     }
     if constexpr (DIAG) {   // warp shuffles, then the block's warps in order
@@ -633,7 +634,8 @@ constexpr int ZWS_NPH = 9, ZWS_NOUT = 4;
 template <typename T, int N, int NPH, int NRAW>
 __global__ void __launch_bounds__((ZWS_NPH + ZWS_NOUT) * 32, 2)
 k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
-      int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err) {
+      int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err,
+      long long mpairs, long long ms) {
     static_assert(NPH == ZWS_NPH && sizeof(T) == 4, "k_zws serves FP32 with 9 physical quantities");
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
@@ -670,7 +672,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
         if (!withhold)
-            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + p * rawf, raw_bytes, bar);
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset(p, mpairs, ms, rawf), raw_bytes, bar);
     };
     if (threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
@@ -707,7 +709,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
             for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
             __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
-            zr_store_r2c<T, N>(lane, x, scr, f.p[warp - NPH] + prev * rawf, ncp);
+            zr_store_r2c<T, N>(lane, x, scr, f.p[warp - NPH] + pair_offset(prev, mpairs, ms, rawf), ncp);
         }
         __syncthreads();   // quantities of `pair` in the inverse warps' lines; the forward lines are free
         if (stop) {

@@ -65,6 +65,40 @@ def test_ensemble_members_match_alone(torch_cuda):
 
 
 @pytest.mark.gpu
+def test_ensemble_batched_groups_match_alone(torch_cuda):
+    """Members of one geometry are stepped by one batched launch per stage
+    (gnss_step_batch); each keeps its own Reynolds and Schmidt numbers and
+    time step, and ends bit-identical to the same jet run alone.  Groups:
+    3 x 32^3 FP64, 4 x 24 x 32 x 16 FP32 with two scalars, 2 x 16^3 FP64
+    with the colloid drift, and one 16^3 member of another drift coefficient
+    (a group of its own)."""
+    import gnss_b200 as G
+    cfgs = [G.make_config(32, re=re, sc=sc, dt=dt) for re, sc, dt in ((500.0, 0.7, 2e-3), (900.0, 1.0, 1e-3),
+                                                                       (1500.0, 2.0, 1.5e-3))]
+    cfgs += [G.make_config(nx=24, ny=32, nz=16, re=re, sc=0.7, sc_c=scc, dt=1e-3, n_scalars=2,
+                           precision=G.GNSS_FP32) for re, scc in ((700.0, 1.0), (1100.0, 2.0), (1600.0, 0.5),
+                                                                  (2500.0, 1.0))]
+    cfgs += [G.make_config(16, re=re, sc=0.7, sc_c=1.0, alpha=0.05, dt=2e-3, n_scalars=2) for re in (300.0, 600.0)]
+    cfgs += [G.make_config(16, re=400.0, sc=0.7, sc_c=1.0, alpha=0.02, dt=2e-3, n_scalars=2)]
+    init = [_init(G, c, seed=20 + i) for i, c in enumerate(cfgs)]
+    with G.Ensemble(cfgs, n_branches=2) as ens:
+        for i, a in enumerate(init):
+            ens.upload(i, a)
+        ens.step(1)
+        ens.step(4)
+        ens.step(4)
+        assert ens.launches_per_step() == 6 * 4   # four groups, six launches each
+        got = []
+        for i, a in enumerate(init):
+            out = np.empty_like(a)
+            ens.download(i, out)
+            got.append(out)
+    for i, (c, a) in enumerate(zip(cfgs, init)):
+        ref, _ = _alone(G, c, a, 9)
+        assert np.array_equal(got[i], ref), f"member {i} differs from the jet run alone"
+
+
+@pytest.mark.gpu
 def test_ensemble_autotune_keeps_results(torch_cuda):
     import gnss_b200 as G
     cfgs = [G.make_config(256, re=2000.0, dt=5e-4, precision=G.GNSS_FP32),
@@ -73,7 +107,7 @@ def test_ensemble_autotune_keeps_results(torch_cuda):
     with G.Ensemble(cfgs, n_branches=2) as ens:
         choices = ens.autotune(2)
         zallowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED, G.GNSS_VARIANT_WARPSPEC)
-        pallowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED)
+        pallowed = (G.GNSS_VARIANT_REGISTER, G.GNSS_VARIANT_STAGED, G.GNSS_VARIANT_TENSOR)
         assert all(ch & 3 in zallowed and ch >> 2 in pallowed for ch in choices)
         for i, a in enumerate(init):
             ens.upload(i, a)
