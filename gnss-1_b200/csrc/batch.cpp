@@ -2,13 +2,15 @@
 // gnss_b200.h.
 //
 // Ensemble: many independent jets (uneven grids, Reynolds and Schmidt numbers)
-// stepped together.  Members of one geometry (grid, precision, scalars, the
-// CN/AB2 scheme, drift coefficient) form groups of up to GNSS_BATCH_MAX whose
-// step is one batched launch per stage (gnss_step_batch: their state,
-// history and scratch lie at fixed strides in one buffer per group).  Groups
-// are spread over a few non-blocking streams; the steps of all groups are
-// captured once into one CUDA graph (one branch per stream) and replayed, so
-// a block of steps of the whole ensemble is one launch.
+// stepped together.  Members of one geometry (grid, precision, scalars,
+// scheme, drift coefficient) form groups of up to GNSS_BATCH_MAX whose state,
+// history and scratch lie at fixed strides in one buffer per group.  A group
+// steps either member by member (each member a unit of its own) or, where
+// its kernels allow, as one batched launch per stage (gnss_step_batch: the
+// group is one unit); the autotuner picks per group.  Units are spread over a
+// few non-blocking streams; the steps of all units are captured once into one
+// CUDA graph (one branch per stream) and replayed, so a block of steps of the
+// whole ensemble is one launch.
 //
 // Server: continuous batching.  Submitted requests wait in arrival order; a
 // scheduler thread admits them as soon as an active slot and enough of the
@@ -53,6 +55,7 @@ struct Member {
     void *buf = nullptr;   // state (nf fields) then history (nf fields), in its group's buffer
     gnss_fields state{}, hist{};
     int group = 0;
+    int branch = 0;        // stream of the member's own steps
 };
 
 // Members of one geometry stepped by one batched launch per stage (or, for a
@@ -63,8 +66,8 @@ struct Group {
     void *scratch = nullptr;   // the members' scratch slices
     size_t slot = 0;           // bytes per member slot (state + history), a multiple of 256
     size_t slice = 0;          // bytes per member scratch slice, a multiple of 256
-    bool batched = false;
-    int branch = 0;
+    bool batched = false;      // one batched launch per stage (else the members' own steps)
+    int branch = 0;            // stream of the batched steps
     double points = 0.0;
     long long launches_per_step = 0;
 };
@@ -110,6 +113,32 @@ static void ensemble_free(gnss_ensemble *e) {
     delete e;
 }
 
+// Units (a batched group, or a member stepping on its own) to branches: longest
+// processing time first, each unit (by points) to the least-loaded branch.
+static void assign_branches(gnss_ensemble *e) {
+    struct Unit { double pts; int group; int member; };
+    std::vector<Unit> units;
+    for (size_t gi = 0; gi < e->groups.size(); ++gi) {
+        const Group &g = e->groups[gi];
+        if (g.batched) {
+            units.push_back({g.points, (int)gi, -1});
+        } else {
+            for (int i : g.members) {
+                const gnss_config &c = e->m[i].cfg;
+                units.push_back({(double)c.nx * c.ny * c.nz, -1, i});
+            }
+        }
+    }
+    std::stable_sort(units.begin(), units.end(), [](const Unit &a, const Unit &b) { return a.pts > b.pts; });
+    std::vector<double> load(e->nbranch, 0.0);
+    for (const Unit &u : units) {
+        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        if (u.group >= 0) e->groups[u.group].branch = b;
+        else e->m[u.member].branch = b;
+        load[b] += u.pts;
+    }
+}
+
 gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n, int nbranch, gnss_ensemble **out) {
     if (!cfgs || !out || n < 1 || nbranch < 1) return GNSS_ERR_INVALID;
     *out = nullptr;
@@ -139,7 +168,6 @@ gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n, int nbranch, gn
         if (gi < 0) {
             gi = (int)e->groups.size();
             e->groups.emplace_back();
-            e->groups[gi].batched = mb.cfg.scheme == GNSS_SCHEME_CNAB2;
         }
         e->groups[gi].members.push_back(i);
         mb.group = gi;
@@ -174,18 +202,8 @@ gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n, int nbranch, gn
         ensemble_free(e);
         return st;
     }
-    // longest processing time first: each group (by points) to the least-loaded branch
-    e->nbranch = std::min(nbranch, (int)e->groups.size());
-    std::vector<int> order(e->groups.size());
-    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return e->groups[a].points > e->groups[b].points; });
-    std::vector<double> load(e->nbranch, 0.0);
-    for (int gi : order) {
-        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        e->groups[gi].branch = b;
-        load[b] += e->groups[gi].points;
-    }
+    e->nbranch = std::min(nbranch, n);
+    assign_branches(e);
     e->streams.assign(e->nbranch, nullptr);
     e->ev_join.assign(e->nbranch, nullptr);
     for (int b = 0; b < e->nbranch && st == GNSS_OK; ++b) {
@@ -258,19 +276,35 @@ long long gnss_ensemble_launches_per_step(const gnss_ensemble *e) {
     return s;
 }
 
-// Group g's step as the ensemble runs it (one batched step, or the members'
-// own steps), on the group's branch stream.
-static gnss_status group_step(gnss_ensemble *e, Group &g, int euler, cudaStream_t bs) {
-    gnss_ctx *ctxs[GNSS_BATCH_MAX];
-    for (size_t j = 0; j < g.members.size(); ++j) ctxs[j] = e->m[g.members[j]].ctx;
+// Group g's step as the ensemble runs it: one batched step on the group's
+// branch (where its kernels allow), or each member's own step on the member's
+// branch.
+static gnss_status group_step(gnss_ensemble *e, Group &g, int euler) {
     const Member &m0 = e->m[g.members[0]];
-    if (g.batched)
+    if (g.batched && gnss_batch_supported(m0.ctx)) {
+        gnss_ctx *ctxs[GNSS_BATCH_MAX];
+        for (size_t j = 0; j < g.members.size(); ++j) ctxs[j] = e->m[g.members[j]].ctx;
         return gnss_step_batch(ctxs, (int)g.members.size(), &m0.state, &m0.hist, g.slot, g.scratch, g.slice, euler,
-                               bs);
+                               e->streams[g.branch]);
+    }
     for (int i : g.members) {
         Member &mb = e->m[i];
-        gnss_status st = gnss_step(mb.ctx, &mb.state, &mb.hist, euler, bs);
+        gnss_status st = gnss_step(mb.ctx, &mb.state, &mb.hist, euler, e->streams[mb.branch]);
         if (st) return st;
+    }
+    return GNSS_OK;
+}
+
+static gnss_status fork_branches(gnss_ensemble *e, cudaStream_t s) {
+    if (cudaEventRecord(e->ev_fork, s) != cudaSuccess) return GNSS_ERR_CUDA;
+    for (int b = 0; b < e->nbranch; ++b)
+        if (cudaStreamWaitEvent(e->streams[b], e->ev_fork, 0) != cudaSuccess) return GNSS_ERR_CUDA;
+    return GNSS_OK;
+}
+static gnss_status join_branches(gnss_ensemble *e, cudaStream_t s) {
+    for (int b = 0; b < e->nbranch; ++b) {
+        if (cudaEventRecord(e->ev_join[b], e->streams[b]) != cudaSuccess) return GNSS_ERR_CUDA;
+        if (cudaStreamWaitEvent(s, e->ev_join[b], 0) != cudaSuccess) return GNSS_ERR_CUDA;
     }
     return GNSS_OK;
 }
@@ -284,25 +318,18 @@ static bool has_tensor_pass(const gnss_config &c) {
 // joined back into stream `s`: one batched step per group, or the members'
 // own steps one after another.
 static gnss_status ensemble_issue(gnss_ensemble *e, int n_steps, int euler_first, cudaStream_t s) {
-    if (cudaEventRecord(e->ev_fork, s) != cudaSuccess) return GNSS_ERR_CUDA;
-    for (int b = 0; b < e->nbranch; ++b)
-        if (cudaStreamWaitEvent(e->streams[b], e->ev_fork, 0) != cudaSuccess) return GNSS_ERR_CUDA;
+    gnss_status st = fork_branches(e, s);
+    if (st) return st;
     for (Group &g : e->groups) {
-        const cudaStream_t bs = e->streams[g.branch];
         for (int k = 0; k < n_steps; ++k) {
             long long l0 = 0, l1 = 0;
             for (int i : g.members) l0 += gnss_launch_count(e->m[i].ctx);
-            gnss_status st = group_step(e, g, (euler_first && k == 0) ? 1 : 0, bs);
-            if (st) return st;
+            if ((st = group_step(e, g, (euler_first && k == 0) ? 1 : 0))) return st;
             for (int i : g.members) l1 += gnss_launch_count(e->m[i].ctx);
             g.launches_per_step = l1 - l0;
         }
     }
-    for (int b = 0; b < e->nbranch; ++b) {
-        if (cudaEventRecord(e->ev_join[b], e->streams[b]) != cudaSuccess) return GNSS_ERR_CUDA;
-        if (cudaStreamWaitEvent(s, e->ev_join[b], 0) != cudaSuccess) return GNSS_ERR_CUDA;
-    }
-    return GNSS_OK;
+    return join_branches(e, s);
 }
 
 static gnss_status ensemble_capture(gnss_ensemble *e, int n_steps) {
@@ -346,6 +373,23 @@ gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream) {
     return GNSS_OK;
 }
 
+gnss_status gnss_ensemble_set_batching(gnss_ensemble *e, int on) {
+    if (!e) return GNSS_ERR_INVALID;
+    for (Group &g : e->groups) g.batched = on != 0 && gnss_batch_supported(e->m[g.members[0]].ctx);
+    assign_branches(e);
+    if (e->gexec) {   // the next block of steps is captured anew
+        cudaGraphExecDestroy(e->gexec);
+        e->gexec = nullptr;
+    }
+    return GNSS_OK;
+}
+
+int gnss_ensemble_batched(const gnss_ensemble *e, int i) {
+    if (!e || i < 0 || i >= (int)e->m.size()) return -1;
+    const Group &g = e->groups[e->m[i].group];
+    return g.batched && gnss_batch_supported(e->m[g.members[0]].ctx) ? 1 : 0;
+}
+
 gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     if (!e || steps < 1) return GNSS_ERR_INVALID;
     if (cudaSetDevice(e->device) != cudaSuccess) return GNSS_ERR_CUDA;
@@ -356,14 +400,17 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
     const int zvariants[3] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED, GNSS_VARIANT_WARPSPEC};
     const int pvariants[3] = {GNSS_VARIANT_REGISTER, GNSS_VARIANT_STAGED, GNSS_VARIANT_TENSOR};
     std::vector<int> best(e->groups.size(), GNSS_VARIANT_AUTO);
+    std::vector<bool> best_batched(e->groups.size(), false);
+    const cudaStream_t ts = e->cap;   // timing stream: the group's steps fork from it and join back
     for (size_t gi = 0; gi < e->groups.size() && !st; ++gi) {
         Group &g = e->groups[gi];
         const Member &m0 = e->m[g.members[0]];
-        const cudaStream_t bs = e->streams[g.branch];
         float tbest = 0.f;
         int vbest = -1;
-        for (int combo = 0; combo < 9; ++combo) {
-            const int zv = zvariants[combo % 3], pv = pvariants[combo / 3];
+        bool bbest = false;
+        for (int combo = 0; combo < 18 && !st; ++combo) {
+            const int zv = zvariants[combo % 3], pv = pvariants[(combo / 3) % 3];
+            const bool batched = combo >= 9;   // the same kernels, as one batched launch per stage
             if (pv == GNSS_VARIANT_TENSOR && !has_tensor_pass(m0.cfg)) continue;
             const int v = zv + 4 * pv;   // z variant + 4 * pass variant
             for (int i : g.members)
@@ -374,24 +421,33 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
             int zk = 0;
             if (zv == GNSS_VARIANT_WARPSPEC && (gnss_get_option(m0.ctx, GNSS_OPT_ZKERNEL, &zk) || zk != zv))
                 continue;   // no warp-specialised kernel here: the same kernels as the register choice
-            if ((st = group_step(e, g, 1, bs))) break;   // warm-up
-            cudaEventRecord(t0, bs);
-            for (int i = 0; i < steps && !st; ++i) st = group_step(e, g, 0, bs);
-            cudaEventRecord(t1, bs);
-            if (st) break;
+            if (batched && (g.members.size() < 2 || !gnss_batch_supported(m0.ctx))) continue;
+            g.batched = batched;
+            if ((st = fork_branches(e, ts)) || (st = group_step(e, g, 1)) || (st = join_branches(e, ts)))
+                break;   // warm-up
+            cudaEventRecord(t0, ts);
+            if ((st = fork_branches(e, ts))) break;
+            for (int i = 0; i < steps && !st; ++i) st = group_step(e, g, 0);
+            if (st || (st = join_branches(e, ts))) break;
+            cudaEventRecord(t1, ts);
             cudaEventSynchronize(t1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, t0, t1);
             if (vbest < 0 || ms < tbest) {
                 tbest = ms;
                 vbest = v;
+                bbest = batched;
             }
         }
-        if (!st) best[gi] = vbest;
+        if (!st) {
+            best[gi] = vbest;
+            best_batched[gi] = bbest;
+        }
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (st) return st;
+    for (size_t gi = 0; gi < e->groups.size(); ++gi) e->groups[gi].batched = best_batched[gi];
     for (size_t i = 0; i < e->m.size(); ++i) {
         Member &mb = e->m[i];
         const int v = best[mb.group];
@@ -402,6 +458,7 @@ gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices) {
         const size_t fb = field_bytes_of(mb.cfg);
         if (cudaMemset(mb.buf, 0, 2 * nfields_of(mb.cfg) * fb) != cudaSuccess) return GNSS_ERR_CUDA;
     }
+    assign_branches(e);
     if (cudaDeviceSynchronize() != cudaSuccess) return GNSS_ERR_CUDA;
     if (e->gexec) {
         cudaGraphExecDestroy(e->gexec);

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <type_traits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -189,33 +190,58 @@ __host__ __device__ constexpr bool zr_auto_pass(int n, bool fp64) {
     return zr_size(n) && (fp64 ? n >= 256 : n != 64);
 }
 
+template <typename T> static const V2<T> *pass_twiddles(const PassPtrs<T> &, const void *tw) {
+    return reinterpret_cast<const V2<T> *>(tw);
+}
+
+// A persistent pass launch: one block per SM times the blocks that fit
+// (looked up once per kernel, from any host thread), at most one per work item.
+template <class K, class PP>
+static cudaError_t launch_persistent(K kern, std::atomic<int> &per_sm, int nt, int smem, int nsm, long long nitems,
+                                     cudaStream_t s, const PP &P, const PassSpec &sp, const void *tw,
+                                     unsigned *err = nullptr, bool with_err = false) {
+    cudaError_t e = prep_smem(kern, smem);
+    if (e != cudaSuccess) return e;
+    int ps = per_sm.load(std::memory_order_relaxed);
+    if (ps == 0) {
+        ps = blocks_per_sm(kern, nt, smem);
+        per_sm.store(ps, std::memory_order_relaxed);
+    }
+    long long grid = (long long)ps * nsm;
+    if (grid > nitems) grid = nitems;
+    if (with_err) {
+        if constexpr (std::is_invocable_v<K, PP, PassSpec, const float2 *, unsigned *>)
+            kern<<<(unsigned)grid, nt, smem, s>>>(P, sp, reinterpret_cast<const float2 *>(tw), err);
+    } else {
+        if constexpr (!std::is_invocable_v<K, PP, PassSpec, const float2 *, unsigned *>)
+            kern<<<(unsigned)grid, nt, smem, s>>>(P, sp, pass_twiddles(P, tw));
+    }
+    return cudaGetLastError();
+}
+
 template <typename T, int N> struct Launch {
+    // Members of a batch (sp.nmem > 1) run the MB instantiations, which exist for the register lengths
+    // (N = 64 .. 512); other lengths return cudaErrorNotSupported for a batch.
     static cudaError_t pass(int sign, const PassPtrs<T> &P, const PassSpec &sp, const void *tw, int nsm,
                             cudaStream_t s, int pvariant, unsigned *err) {
+        const bool mb = sp.nmem > 1;
+        const int ci = (sign < 0 ? 0 : 1) + (mb ? 2 : 0);   // occupancy cache index
         if constexpr (sizeof(T) == 4 && ptc_size(N)) {
             // split-TF32 DFT-GEMM transforms on the tensor cores (tiles of 8 columns)
             if (pvariant == GNSS_VARIANT_TENSOR) {
                 using C = PTCfg<N>;
-                auto kern = sign < 0 ? k_passtc<N, -1> : k_passtc<N, +1>;
-                cudaError_t e = prep_smem(kern, C::SMEM);
-                if (e != cudaSuccess) return e;
-                static std::atomic<int> per_sm[2];   // resident blocks per SM, looked up once (any thread)
-                int ps = per_sm[sign < 0 ? 0 : 1].load(std::memory_order_relaxed);
-                if (ps == 0) {
-                    ps = blocks_per_sm(kern, C::NT, C::SMEM);
-                    per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
-                }
+                auto kern = mb ? (sign < 0 ? k_passtc<N, -1, true> : k_passtc<N, +1, true>)
+                               : (sign < 0 ? k_passtc<N, -1> : k_passtc<N, +1>);
+                static std::atomic<int> per_sm[4];
                 PassSpec s8 = sp;
                 const int cols = sp.ncols > sp.out_ncols ? sp.ncols : sp.out_ncols;
                 s8.ncolblk = (cols + C::NB - 1) / C::NB;
                 const long long nitems = (long long)s8.nmem * s8.nin * s8.outer.count() * s8.ncolblk;
-                long long grid = (long long)ps * nsm;
-                if (grid > nitems) grid = nitems;
-                kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(reinterpret_cast<const PassPtrs<float> &>(P), s8,
-                                                            reinterpret_cast<const float2 *>(tw), err);
-                return cudaGetLastError();
+                return launch_persistent(kern, per_sm[ci], C::NT, C::SMEM, nsm, nitems, s,
+                                         reinterpret_cast<const PassPtrs<float> &>(P), s8, tw, err, true);
             }
         }
+        const long long nitems = (long long)sp.nmem * sp.nin * sp.outer.count() * sp.ncolblk;
         if constexpr (zr_size(N)) {
             // register-resident column transforms where they measured faster (512^3 FP32 step 7.34 against
             // 8.39 ms, FP64 10.1 against 8.9 Gpoint-steps/s; 256^3 1.23 against 1.28 ms; N = 96 .. 192 with
@@ -225,37 +251,24 @@ template <typename T, int N> struct Launch {
                               zr_auto_pass(N, sizeof(T) == 8));
             if (reg) {
                 using C = PRCfg<T, N>;
-                auto kern = sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>;
-                cudaError_t e = prep_smem(kern, C::SMEM);
-                if (e != cudaSuccess) return e;
-                static std::atomic<int> per_sm[2];   // resident blocks per SM, looked up once (any thread)
-                int ps = per_sm[sign < 0 ? 0 : 1].load(std::memory_order_relaxed);
-                if (ps == 0) {
-                    ps = blocks_per_sm(kern, C::NT, C::SMEM);
-                    per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
-                }
-                const long long nitems = (long long)sp.nmem * sp.nin * sp.outer.count() * sp.ncolblk;
-                long long grid = (long long)ps * nsm;
-                if (grid > nitems) grid = nitems;
-                kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(P, sp, reinterpret_cast<const V2<T> *>(tw));
-                return cudaGetLastError();
+                auto kern = mb ? (sign < 0 ? k_passr<T, N, -1, true> : k_passr<T, N, +1, true>)
+                               : (sign < 0 ? k_passr<T, N, -1> : k_passr<T, N, +1>);
+                static std::atomic<int> per_sm[4];
+                return launch_persistent(kern, per_sm[ci], C::NT, C::SMEM, nsm, nitems, s, P, sp, tw);
             }
         }
         using C = PassCfg<T, N>;
-        auto kern = sign < 0 ? k_pass<T, N, -1> : k_pass<T, N, +1>;
-        cudaError_t e = prep_smem(kern, C::SMEM);
-        if (e != cudaSuccess) return e;
-        static std::atomic<int> per_sm[2];   // resident blocks per SM, looked up once (any thread)
-        int ps = per_sm[sign < 0 ? 0 : 1].load(std::memory_order_relaxed);
-        if (ps == 0) {
-            ps = blocks_per_sm(kern, C::NT, C::SMEM);
-            per_sm[sign < 0 ? 0 : 1].store(ps, std::memory_order_relaxed);
+        static std::atomic<int> per_sm[4];
+        if (mb) {
+            if constexpr (zr_size(N)) {
+                auto kern = sign < 0 ? k_pass<T, N, -1, true> : k_pass<T, N, +1, true>;
+                return launch_persistent(kern, per_sm[ci], C::NT, C::SMEM, nsm, nitems, s, P, sp, tw);
+            } else {
+                return cudaErrorNotSupported;
+            }
         }
-        const long long nitems = (long long)sp.nmem * sp.nin * sp.outer.count() * sp.ncolblk;
-        long long grid = (long long)ps * nsm;
-        if (grid > nitems) grid = nitems;
-        kern<<<(unsigned)grid, C::NT, C::SMEM, s>>>(P, sp, reinterpret_cast<const V2<T> *>(tw));
-        return cudaGetLastError();
+        auto kern = sign < 0 ? k_pass<T, N, -1> : k_pass<T, N, +1>;
+        return launch_persistent(kern, per_sm[ci], C::NT, C::SMEM, nsm, nitems, s, P, sp, tw);
     }
     static cudaError_t zpass(int dir, const FieldSet<T> &f, int nfields, long long nlines, int nz2, T scale,
                              const void *tw, cudaStream_t s) {
@@ -273,6 +286,7 @@ template <typename T, int N> struct Launch {
     static cudaError_t zphys_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
                                int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
                                cudaStream_t s, int nmem, long long ms) {
+        if (nmem > 1) return cudaErrorNotSupported;   // batches run the register z kernel
         using C = ZPCfg<T, N>;
         const int pipe_b = C::pipe_bytes(NPH, NRAW, ncp, PP);
         const int pipe = pipe_b <= C::SMEM_MAX ? 1 : 0;
@@ -308,7 +322,8 @@ template <typename T, int N> struct Launch {
         if constexpr (zr_size(N)) {
             const int smem = ZRCfg<T, N>::smem_bytes(NPH, NRAW, ncp);
             if (smem > ZPCfg<T, N>::SMEM_MAX) return cudaErrorNotSupported;
-            auto kern = diag ? k_zreg<T, N, NPH, NRAW, true> : k_zreg<T, N, NPH, NRAW, false>;
+            auto kern = diag ? k_zreg<T, N, NPH, NRAW, true>
+                             : (nmem > 1 ? k_zreg<T, N, NPH, NRAW, false, true> : k_zreg<T, N, NPH, NRAW, false>);
             cudaError_t e = prep_smem(kern, smem);
             if (e != cudaSuccess) return e;
             const int per_sm = blocks_per_sm(kern, NPH * 32, smem);
@@ -329,6 +344,7 @@ template <typename T, int N> struct Launch {
     static cudaError_t zws_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
                              T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s,
                              int nmem, long long ms) {
+        if (nmem > 1) return cudaErrorNotSupported;   // batches run the register z kernel
         if constexpr ((N == 256 || N == 512) && sizeof(T) == 4) {
             const int smem = ZRCfg<T, N>::smem_bytes_ws(ZWS_NPH, ZWS_NOUT, 10, ncp);
             auto kern = k_zws<T, N, ZWS_NPH, 10>;
@@ -1617,12 +1633,19 @@ static gnss_status step_batch_t(gnss_ctx *const *cs, int n, const gnss_fields *s
     return nonlinear_and_update<T>(c, st0, nullptr, hi0, uc, s, nullptr, nullptr, bt);
 }
 
+bool gnss_batch_supported(const gnss_ctx *c) {
+    if (!c || c->cfg.scheme != GNSS_SCHEME_CNAB2) return false;
+    const int zk = c->cfg.precision == GNSS_FP64 ? zkernel_of<double>(c) : zkernel_of<float>(c);
+    return zk == GNSS_VARIANT_REGISTER && zr_size(c->g.nx) && zr_size(c->g.ny);
+}
+
 gnss_status gnss_step_batch(gnss_ctx *const *cs, int n, const gnss_fields *st0, const gnss_fields *hi0,
                             size_t member_bytes, void *scratch, size_t scratch_bytes, int euler, void *stream) {
     if (!cs || n < 1 || n > GNSS_BATCH_MAX || !cs[0] || !scratch) return GNSS_ERR_INVALID;
     gnss_ctx *c = cs[0];
     const gnss_config &k = c->cfg;
-    if (k.scheme != GNSS_SCHEME_CNAB2) return fail(c, GNSS_ERR_UNSUPPORTED, "batched steps use the CN/AB2 scheme");
+    if (!gnss_batch_supported(c))
+        return fail(c, GNSS_ERR_UNSUPPORTED, "batched steps need the CN/AB2 scheme and the register kernels");
     for (int m = 1; m < n; ++m) {
         const gnss_config &o = cs[m] ? cs[m]->cfg : k;
         if (!cs[m] || o.nx != k.nx || o.ny != k.ny || o.nz != k.nz || o.precision != k.precision ||

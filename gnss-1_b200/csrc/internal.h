@@ -12,6 +12,10 @@ constexpr int GNSS_BATCH_MAX = 16;
 // intermediates of the context's geometry).
 size_t gnss_batch_scratch_bytes(const gnss_ctx *ctx);
 
+// Whether a context's kernel choices allow batched steps: the register z
+// kernel and x / y lengths with register passes (64 .. 512).
+bool gnss_batch_supported(const gnss_ctx *ctx);
+
 // One fused step of n members of one geometry (grid, precision, scalar count,
 // the CN/AB2 scheme, drift coefficient) in one launch per stage.  Member m's
 // state and history fields lie m * member_bytes after state0's and hist0's;

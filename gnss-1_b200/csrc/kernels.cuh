@@ -136,7 +136,7 @@ __device__ __forceinline__ void tile_prefetch(V2<T> *dst, const V2<T> *__restric
 
 // Persistent: block b handles items b, b + gridDim.x, ... and prefetches the
 // next item's tile while transforming the current one.
-template <typename T, int N, int SIGN>
+template <typename T, int N, int SIGN, bool MB = false>
 __global__ void __launch_bounds__(PassCfg<T, N>::NT, 1)
 k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec sp, const V2<T> *__restrict__ tw) {
     using V = V2<T>;
@@ -148,15 +148,15 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
     const int tid = threadIdx.x;
     const int ntiles = sp.outer.count() * sp.ncolblk;
     const int mitems = sp.nin * ntiles;   // items of one member
-    const long long nitems = (long long)sp.nmem * mitems;
+    const long long nitems = MB ? (long long)sp.nmem * mitems : (long long)mitems;
     long long item = blockIdx.x;
     if (item >= nitems) return;
-    // mi: member, oc: compact outer index, o: expanded outer index
+    // mi: member (MB: a batch of members), oc: compact outer index, o: expanded outer index
     // work items fit in 32 bits (members x inputs x outer indices x column blocks): 32-bit divisions
     auto decode = [&](long long it, int &mi, int &fi, int &oc, int &o, int &c0) {
         const int i32 = (int)it;
-        mi = i32 / mitems;
-        const int r = i32 - mi * mitems;
+        mi = MB ? i32 / mitems : 0;
+        const int r = MB ? i32 - mi * mitems : i32;
         fi = r / ntiles;
         const int t = r - fi * ntiles;
         oc = t / sp.ncolblk;
@@ -166,7 +166,7 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
     auto prefetch = [&](long long it, V *dst) {
         int mi, fi, oc, o, c0;
         decode(it, mi, fi, oc, o, c0);
-        const V *src = P.in[fi] + mi * sp.ms_in + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        const V *src = P.in[fi] + (MB ? mi * sp.ms_in : 0LL) + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
         tile_prefetch<T, NB, NT, TILE>(dst, src, sp, c0, tid);
     };
     prefetch(item, rawb[0]);
@@ -182,7 +182,7 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
         decode(item, mi, fi, oc, o, c0);
         const V *cur = rawb[buf];
         const double k_out = sp.n_out ? wavenum(o, sp.n_out, sp.dk_out) : 0.0;
-        const long long dbase = mi * sp.ms_out + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const long long dbase = (MB ? mi * sp.ms_out : 0LL) + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0;
         const int nv = sp.nvar[fi];
         for (int v = 0; v < nv; ++v) {
@@ -351,15 +351,20 @@ k_zpass(FieldSet<T> f, long long nlines, int nz2, T scale, const V2<T> *__restri
 //   4 alpha (lap s c + grad c . grad s) + u . grad c   (colloidAdvectionKernel_mgpu, solver.cu:374-388)
 // One warp per input field; one block per line pair.
 //
-// Batches: the line pairs of nmem members of one geometry are numbered
-// member after member (mpairs per member), and a member's fields lie ms
-// elements after the previous member's; pair p of the batch starts at
-// element pair_offset(p) of each field pointer.  The batch holds fewer than
-// 2^31 pairs.
+// Batches (the MB instantiations): the line pairs of nmem members of one
+// geometry are numbered member after member (mpairs per member), and a
+// member's fields lie ms elements after the previous member's; pair p of the
+// batch starts at element pair_offset(p) of each field pointer.  The batch
+// holds fewer than 2^31 pairs.
+template <bool MB>
 __device__ __forceinline__ long long pair_offset(long long p, long long mpairs, long long ms, int rawf) {
-    const int pi = (int)p, mp = (int)mpairs;
-    const int mi = pi / mp;
-    return mi * ms + (long long)(pi - mi * mp) * rawf;
+    if constexpr (MB) {
+        const int pi = (int)p, mp = (int)mpairs;
+        const int mi = pi / mp;
+        return mi * ms + (long long)(pi - mi * mp) * rawf;
+    } else {
+        return p * rawf;
+    }
 }
 
 template <typename T, int N> struct ZPCfg {
@@ -484,7 +489,7 @@ __device__ __forceinline__ void zphys_products(const V2<T> *reg, V2<T> *out, T s
 // line transforms ping-pong between two banks of lines (one butterfly per
 // lane at a time: fewer registers, more resident warps); otherwise they run
 // in place.  A wait that times out sets bit 0 of *err and the block stops.
-template <typename T, int N, int NPH, int NRAW, bool PP>
+template <typename T, int N, int NPH, int NRAW, bool PP, bool MB = false>
 __global__ void __launch_bounds__(NPH * 32, (PP && sizeof(T) == 4) ? 2 : 1)
 k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
         int ncp, int nkz, int pipe, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw,
@@ -518,7 +523,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
         if (!withhold)
-            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset(p, mpairs, ms, rawf), raw_bytes, bar);
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset<MB>(p, mpairs, ms, rawf), raw_bytes, bar);
     };
     if (pipe && threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
@@ -537,8 +542,8 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
             a0 = raw + rc.r[0] * rawf;
             a1 = rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr;
         } else {
-            a0 = f.p[rc.r[0]] + pair_offset(pair, mpairs, ms, rawf);
-            a1 = rc.r[1] >= 0 ? f.p[rc.r[1]] + pair_offset(pair, mpairs, ms, rawf) : nullptr;
+            a0 = f.p[rc.r[0]] + pair_offset<MB>(pair, mpairs, ms, rawf);
+            a1 = rc.r[1] >= 0 ? f.p[rc.r[1]] + pair_offset<MB>(pair, mpairs, ms, rawf) : nullptr;
         }
         pack_c2r_combo<T, N>(lane, lineA, rc, a0, a1, ncp, nkz, dkz);
         __syncthreads();   // staging area (or the raw lines in global memory) consumed
@@ -559,7 +564,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
             V *pl = prod + warp * LEN;
             if constexpr (PP) warp_line_fft_pp<T, N, -1>(lane, pl, (prod == bankA ? bankB : bankA) + warp * LEN, tw);
             else warp_line_fft<T, N, -1>(lane, pl, tw);
-            V *d = f.p[warp] + pair_offset(pair, mpairs, ms, rawf);
+            V *d = f.p[warp] + pair_offset<MB>(pair, mpairs, ms, rawf);
             unpack_r2c_pad<T, N>(lane, 32, fres + warp * LEN, d, d + ncp, ncp);
         }
         __syncthreads();   // work area reused by the next pair

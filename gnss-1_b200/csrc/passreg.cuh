@@ -64,7 +64,7 @@ template <typename T, int N> __device__ __forceinline__ int pr_tile_row(int r) {
 // |row index| of a transform row (the Nyquist row counts as N/2)
 template <int N> __device__ __forceinline__ int row_dist(int r) { return r <= N / 2 ? r : N - r; }
 
-template <typename T, int N, int SIGN>
+template <typename T, int N, int SIGN, bool MB = false>
 __global__ void __launch_bounds__(PRCfg<T, N>::NT, (N <= 192 && sizeof(T) == 4) ? 2 : 1)
 k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec sp, const V2<T> *__restrict__ tw) {
     using V = V2<T>;
@@ -79,7 +79,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = sp.outer.count() * sp.ncolblk;
     const int mitems = sp.nin * ntiles;   // items of one member
-    const long long nitems = (long long)sp.nmem * mitems;
+    const long long nitems = MB ? (long long)sp.nmem * mitems : (long long)mitems;
     long long item = blockIdx.x;
     if (item >= nitems) return;
     for (int i = tid; i < C::TWR * 32; i += NT) tws[i] = tw[Z::tw_index(i, true)];
@@ -87,8 +87,8 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     // 32-bit divisions
     auto decode = [&](long long it, int &mi, int &fi, int &oc, int &o, int &c0) {
         const int i32 = (int)it;
-        mi = i32 / mitems;
-        const int r = i32 - mi * mitems;
+        mi = MB ? i32 / mitems : 0;   // member of a batch (MB)
+        const int r = MB ? i32 - mi * mitems : i32;
         fi = r / ntiles;
         const int t = r - fi * ntiles;
         oc = t / sp.ncolblk;
@@ -105,7 +105,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
     auto prefetch = [&](long long it, V *dst) {
         int mi, fi, oc, o, c0;
         decode(it, mi, fi, oc, o, c0);
-        const V *src = P.in[fi] + mi * sp.ms_in + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
+        const V *src = P.in[fi] + (MB ? mi * sp.ms_in : 0LL) + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
         const int b = tid % NB;
         if (c0 + b >= sp.ncols) return;
 #pragma unroll 4
@@ -153,7 +153,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             for (int m = 0; m < E; ++m)
                 if (row_dist<N>(lane + 32 * m) > dmax) okm &= ~(1u << m);
         }
-        const long long dbase = mi * sp.ms_out + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const long long dbase = (MB ? mi * sp.ms_out : 0LL) + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0;
         const int nv = sp.nvar[fi];
         for (int v = 0; v < nv; ++v) {

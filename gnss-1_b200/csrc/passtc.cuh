@@ -87,7 +87,7 @@ template <int N> struct PTCfg {
     static_assert(K1 + MT3 * K3 <= (int)TCOLS, "TMEM columns");
 };
 
-template <int N, int SIGN>
+template <int N, int SIGN, bool MB = false>
 __global__ void __launch_bounds__(512, 1)
 k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ PassSpec sp,
          const float2 *__restrict__ tw, unsigned *__restrict__ err) {
@@ -101,7 +101,7 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ntiles = sp.outer.count() * sp.ncolblk;
     const int mitems = sp.nin * ntiles;      // items of one member
-    const int nitems = sp.nmem * mitems;     // < 2^31 (members x inputs x outer indices x column blocks)
+    const int nitems = MB ? sp.nmem * mitems : mitems;   // < 2^31 (members x inputs x outer indices x column blocks)
     int item = blockIdx.x;
     if (item >= nitems) return;   // uniform for the block
     V *twl = reinterpret_cast<V *>(sm + C::OFF_TW);
@@ -156,8 +156,8 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     const WaitCtl wc(err);
 
     auto decode = [&](int it, int &mi, int &fi, int &oc, int &o, int &c0) {
-        mi = it / mitems;
-        const int r = it - mi * mitems;
+        mi = MB ? it / mitems : 0;   // member of a batch (MB)
+        const int r = MB ? it - mi * mitems : it;
         fi = r / ntiles;
         const int t = r - fi * ntiles;
         oc = t / sp.ncolblk;
@@ -181,7 +181,7 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     auto load = [&](int it_item) {
         int mi, fi, oc, o, c0;
         decode(it_item, mi, fi, oc, o, c0);
-        const V *src = P.in[fi] + mi * sp.ms_in + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0 + pc;
+        const V *src = P.in[fi] + (MB ? mi * sp.ms_in : 0LL) + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0 + pc;
         const bool col_ok = c0 + pc < sp.ncols;
 #pragma unroll
         for (int it = 0; it < NIT; ++it)
@@ -370,7 +370,7 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
             }
             __syncthreads();
         }
-        const long long dbase = mi * sp.ms_out + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
+        const long long dbase = (MB ? mi * sp.ms_out : 0LL) + (long long)(sp.outer_out_compact ? oc : o) * sp.d_out + c0;
         const int out_cols = sp.out_ncols - c0 < NB ? sp.out_ncols - c0 : NB;
         const int nv = sp.nvar[fi];
         const int next = item + gridDim.x;

@@ -524,7 +524,7 @@ __device__ __forceinline__ void zr_store_r2c(int lane, const V2<T> *x, V2<T> *sc
 // With DIAG the block also writes one row of ZR_VORT_SUMS vorticity sums over
 // its points to diag[blockIdx.x] (fixed-order reduction), for the statistics
 // of the state the step starts from.
-template <typename T, int N, int NPH, int NRAW, bool DIAG = false>
+template <typename T, int N, int NPH, int NRAW, bool DIAG = false, bool MB = false>
 __global__ void __launch_bounds__(NPH * 32, (sizeof(T) == 4 && NPH <= 9) ? (N <= 192 ? 4 : 3) : (N <= 192 ? 2 : 1))
 k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
        int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err,
@@ -561,7 +561,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
         if (!withhold)
-            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset(p, mpairs, ms, rawf), raw_bytes, bar);
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset<MB>(p, mpairs, ms, rawf), raw_bytes, bar);
     };
     if (threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
@@ -598,7 +598,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
             for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
             __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
-            zr_store_r2c<T, N>(lane, x, scr, f.p[warp] + pair_offset(pair, mpairs, ms, rawf), ncp);
+            zr_store_r2c<T, N>(lane, x, scr, f.p[warp] + pair_offset<MB>(pair, mpairs, ms, rawf), ncp);
         }
     }
     if constexpr (DIAG) {   // warp shuffles, then the block's warps in order
@@ -631,7 +631,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
 // wait that times out sets bit 0 of *err and the block stops.  FP32 with 9
 // quantities: 13 warps, 72 registers, two blocks per SM.
 constexpr int ZWS_NPH = 9, ZWS_NOUT = 4;
-template <typename T, int N, int NPH, int NRAW>
+template <typename T, int N, int NPH, int NRAW, bool MB = false>
 __global__ void __launch_bounds__((ZWS_NPH + ZWS_NOUT) * 32, 2)
 k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
       int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err,
@@ -672,7 +672,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
         if (!withhold)
-            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset(p, mpairs, ms, rawf), raw_bytes, bar);
+            for (int q = 0; q < NRAW; ++q) bulk_g2s(raw + q * rawf, f.p[q] + pair_offset<MB>(p, mpairs, ms, rawf), raw_bytes, bar);
     };
     if (threadIdx.x == 0) issue(pair, wc.withhold);
     unsigned parity = 0;
@@ -709,7 +709,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
             for (int m = 0; m < E; ++m) x[m] = scr[Z::pidx(lane + 32 * m)];
             __syncwarp();
             zr_fft<T, N, -1>(lane, x, scr, tws);
-            zr_store_r2c<T, N>(lane, x, scr, f.p[warp - NPH] + pair_offset(prev, mpairs, ms, rawf), ncp);
+            zr_store_r2c<T, N>(lane, x, scr, f.p[warp - NPH] + pair_offset<MB>(prev, mpairs, ms, rawf), ncp);
         }
         __syncthreads();   // quantities of `pair` in the inverse warps' lines; the forward lines are free
         if (stop) {

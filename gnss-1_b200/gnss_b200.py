@@ -142,6 +142,8 @@ _SIGS = {
     "gnss_ensemble_step": [_VP, ctypes.c_int, _VP],
     "gnss_ensemble_launches_per_step": [_VP],
     "gnss_ensemble_autotune": [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)],
+    "gnss_ensemble_set_batching": [_VP, ctypes.c_int],
+    "gnss_ensemble_batched": [_VP, ctypes.c_int],
     "gnss_server_create": [_VP, ctypes.POINTER(ctypes.c_void_p)],
     "gnss_server_destroy": [_VP],
     "gnss_server_submit": [_VP, ctypes.POINTER(GnssConfig), _VP, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)],
@@ -643,6 +645,14 @@ class Ensemble:
 
     def launches_per_step(self) -> int:
         return int(self.lib.gnss_ensemble_launches_per_step(self._h))
+
+    def set_batching(self, on: bool) -> None:
+        """Groups of one geometry step as one batched launch per stage (on) or member by member."""
+        self._ck(self.lib.gnss_ensemble_set_batching(self._h, 1 if on else 0), "gnss_ensemble_set_batching")
+
+    def batched(self, i: int) -> bool:
+        """Whether member i's group steps as batched launches."""
+        return int(self.lib.gnss_ensemble_batched(self._h, int(i))) == 1
 
     def autotune(self, steps: int = 3) -> list:
         ch = (ctypes.c_int * len(self.configs))()

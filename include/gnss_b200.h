@@ -296,18 +296,21 @@ gnss_status gnss_attach_scratch(gnss_ctx *ctx, void *scratch, size_t bytes);
  * An ensemble of independent jets (uneven grids, Reynolds and Schmidt
  * numbers) stepped together.  The library owns every member's state and
  * history.  Members of one geometry (grid, box, precision, scalar count,
- * dealiasing, drift coefficient) with the CN/AB2 scheme form groups of up to
- * 16 whose step is ONE launch per stage for the whole group (each member with
- * its own Reynolds and Schmidt numbers and time step; their state, history
- * and scratch lie at fixed strides in one buffer per group); other members
- * form groups of one.  Groups are spread over n_branches streams (largest
- * first, each to the least-loaded branch).  gnss_ensemble_step runs n_steps
- * steps of every member: the first step of a run (Euler, for
- * GNSS_SCHEME_CNAB2) is launched directly, and the rest as ONE CUDA graph
- * launch that holds all groups' steps in parallel branches (captured on
- * first use for that step count, replayed afterwards).  A member's result is
- * bit-identical to stepping it alone with gnss_step.  No counterpart in the
- * reference (one jet per program). */
+ * scheme, dealiasing, drift coefficient) form groups of up to 16 whose state,
+ * history and scratch lie at fixed strides in one buffer per group.  A group
+ * steps member by member, each member with its own launches, or, where its
+ * kernels allow (CN/AB2, the register z kernel and register lengths), as ONE
+ * batched launch per stage for the whole group, each member keeping its own
+ * Reynolds and Schmidt numbers and time step (gnss_ensemble_set_batching, or
+ * the autotuner per group).  The units (batched groups and members stepping
+ * on their own) are spread over n_branches streams (largest first, each to
+ * the least-loaded branch).  gnss_ensemble_step runs n_steps steps of every
+ * member: the first step of a run (Euler, for GNSS_SCHEME_CNAB2) is launched
+ * directly, and the rest as ONE CUDA graph launch that holds every unit's
+ * steps in parallel branches (captured on first use for that step count,
+ * replayed afterwards).  A member's result is bit-identical to stepping it
+ * alone with gnss_step, in either form.  No counterpart in the reference
+ * (one jet per program). */
 typedef struct gnss_ensemble gnss_ensemble;
 gnss_status gnss_ensemble_create(const gnss_config *cfgs, int n_members, int n_branches, gnss_ensemble **out);
 gnss_status gnss_ensemble_destroy(gnss_ensemble *e);
@@ -325,14 +328,22 @@ gnss_status gnss_ensemble_download(gnss_ensemble *e, int i, void *host_state, vo
 gnss_status gnss_ensemble_step(gnss_ensemble *e, int n_steps, void *stream);
 /* Kernels launched per step of the whole ensemble (for launch accounting). */
 long long gnss_ensemble_launches_per_step(const gnss_ensemble *e);
+/* on != 0: every group whose kernels allow it steps as one batched launch per
+ * stage; 0 (the state after creation): every member steps with its own
+ * launches.  No counterpart in the reference. */
+gnss_status gnss_ensemble_set_batching(gnss_ensemble *e, int on);
+/* 1 when member i's group steps as batched launches, 0 when it steps member by
+ * member, -1 for a bad argument. */
+int gnss_ensemble_batched(const gnss_ensemble *e, int i);
 /* Autotuner: for every group, time each kernel variant (GNSS_OPT_*) over
- * `steps` steps of the group as the ensemble runs it (one batched launch per
- * stage), on the members' own buffers (which are zeroed afterwards, so tune
- * before uploading states), and keep the fastest of the z variants REGISTER,
- * STAGED, WARPSPEC by the pass variants REGISTER, STAGED and, where it exists
- * (FP32, an x or y length of 256 or 512), TENSOR.  choices (may be NULL)
- * receives, per member, the chosen GNSS_OPT_ZVARIANT value + 4 * the
- * GNSS_OPT_PVARIANT value. */
+ * `steps` steps of the group as the ensemble runs it, member by member on the
+ * branch streams and, where the kernels allow it, as batched launches, on the
+ * members' own buffers (which are zeroed afterwards, so tune before uploading
+ * states), and keep the fastest form with the fastest of the z variants
+ * REGISTER, STAGED, WARPSPEC by the pass variants REGISTER, STAGED and, where
+ * it exists (FP32, an x or y length of 256 or 512), TENSOR.  choices (may be
+ * NULL) receives, per member, the chosen GNSS_OPT_ZVARIANT value + 4 * the
+ * GNSS_OPT_PVARIANT value; gnss_ensemble_batched reports the form. */
 gnss_status gnss_ensemble_autotune(gnss_ensemble *e, int steps, int *choices);
 
 /* ---------------------------------------------------------------- serving

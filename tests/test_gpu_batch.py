@@ -66,8 +66,8 @@ def test_ensemble_members_match_alone(torch_cuda):
 
 @pytest.mark.gpu
 def test_ensemble_batched_groups_match_alone(torch_cuda):
-    """Members of one geometry are stepped by one batched launch per stage
-    (gnss_step_batch); each keeps its own Reynolds and Schmidt numbers and
+    """With batching on, members of one geometry are stepped by one batched
+    launch per stage; each keeps its own Reynolds and Schmidt numbers and
     time step, and ends bit-identical to the same jet run alone.  Groups:
     3 x 32^3 FP64, 4 x 24 x 32 x 16 FP32 with two scalars, 2 x 16^3 FP64
     with the colloid drift, and one 16^3 member of another drift coefficient
@@ -82,6 +82,8 @@ def test_ensemble_batched_groups_match_alone(torch_cuda):
     cfgs += [G.make_config(16, re=400.0, sc=0.7, sc_c=1.0, alpha=0.02, dt=2e-3, n_scalars=2)]
     init = [_init(G, c, seed=20 + i) for i, c in enumerate(cfgs)]
     with G.Ensemble(cfgs, n_branches=2) as ens:
+        ens.set_batching(True)
+        assert all(ens.batched(i) for i in range(len(cfgs)))
         for i, a in enumerate(init):
             ens.upload(i, a)
         ens.step(1)
