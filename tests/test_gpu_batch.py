@@ -68,18 +68,19 @@ def test_ensemble_members_match_alone(torch_cuda):
 def test_ensemble_batched_groups_match_alone(torch_cuda):
     """With batching on, members of one geometry are stepped by one batched
     launch per stage; each keeps its own Reynolds and Schmidt numbers and
-    time step, and ends bit-identical to the same jet run alone.  Groups:
-    3 x 32^3 FP64, 4 x 24 x 32 x 16 FP32 with two scalars, 2 x 16^3 FP64
-    with the colloid drift, and one 16^3 member of another drift coefficient
-    (a group of its own)."""
+    time step, and ends bit-identical to the same jet run alone.  Groups
+    (register kernels, which the batched form needs): 3 x 64^3 FP64,
+    4 x 64 x 96 x 64 FP32 with two scalars, 2 x 64^3 FP64 with the colloid
+    drift, and one 64^3 member of another drift coefficient (a group of its
+    own)."""
     import gnss_b200 as G
-    cfgs = [G.make_config(32, re=re, sc=sc, dt=dt) for re, sc, dt in ((500.0, 0.7, 2e-3), (900.0, 1.0, 1e-3),
+    cfgs = [G.make_config(64, re=re, sc=sc, dt=dt) for re, sc, dt in ((500.0, 0.7, 2e-3), (900.0, 1.0, 1e-3),
                                                                        (1500.0, 2.0, 1.5e-3))]
-    cfgs += [G.make_config(nx=24, ny=32, nz=16, re=re, sc=0.7, sc_c=scc, dt=1e-3, n_scalars=2,
+    cfgs += [G.make_config(nx=64, ny=96, nz=64, re=re, sc=0.7, sc_c=scc, dt=1e-3, n_scalars=2,
                            precision=G.GNSS_FP32) for re, scc in ((700.0, 1.0), (1100.0, 2.0), (1600.0, 0.5),
                                                                   (2500.0, 1.0))]
-    cfgs += [G.make_config(16, re=re, sc=0.7, sc_c=1.0, alpha=0.05, dt=2e-3, n_scalars=2) for re in (300.0, 600.0)]
-    cfgs += [G.make_config(16, re=400.0, sc=0.7, sc_c=1.0, alpha=0.02, dt=2e-3, n_scalars=2)]
+    cfgs += [G.make_config(64, re=re, sc=0.7, sc_c=1.0, alpha=0.05, dt=2e-3, n_scalars=2) for re in (300.0, 600.0)]
+    cfgs += [G.make_config(64, re=400.0, sc=0.7, sc_c=1.0, alpha=0.02, dt=2e-3, n_scalars=2)]
     init = [_init(G, c, seed=20 + i) for i, c in enumerate(cfgs)]
     with G.Ensemble(cfgs, n_branches=2) as ens:
         ens.set_batching(True)
