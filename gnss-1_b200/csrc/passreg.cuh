@@ -53,12 +53,25 @@ template <typename T, int N> struct ColScratch {
 // lane ends holding rows q + E j (j = bitrev5(lane)); storing row q + E j at
 // tile row 32 q + j makes a warp's stores of one q land in distinct bank
 // pairs (row r itself would put 32 / E lanes on each, with the pitch LD).
+// With the transpose, a warp's stores of one q put lane group j = lane % G on
+// rows E^2 sigma(j) apart (zr_out_index), all on the same banks; rotating
+// block b = r / E^2 of the rows by b RS rows puts the groups that share a
+// wavefront (8 lanes of 16 bytes, 16 of 8) on distinct banks (2x fewer
+// wavefronts for N = 512, 4x for N = 256).  Measured at 512^3 (FP64, two
+// scalars): passes 8.39 -> 8.04 ms per step; at 256^3 FP64 1.39 -> 1.17 ms,
+// FP32 0.756 -> 0.714 ms.  FP32 with N = 512 keeps row r: its conflicts are
+// 2-way and its passes issue-bound, and the rotation made them 4% slower.
 template <typename T, int N> __device__ __forceinline__ int pr_tile_row(int r) {
     using Z = ZRCfg<T, N>;
-    if constexpr (Z::SHFL)
+    if constexpr (Z::SHFL) {
         return (r % Z::E) * 32 + r / Z::E;
-    else
+    } else if constexpr (sizeof(T) == 4 && Z::E == 16) {
         return r;
+    } else {
+        constexpr int B = Z::E * Z::E, RS = Z::E / (sizeof(T) == 8 ? 4 : 2);
+        const int b = r / B;
+        return b * B + (r % B + b * RS) % B;
+    }
 }
 
 // |row index| of a transform row (the Nyquist row counts as N/2)
@@ -187,7 +200,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
                 for (int q = 0; q < E; ++q) col[(32 * q + j) * LD] = x[q];   // pr_tile_row(q + E j)
             } else {
 #pragma unroll
-                for (int q = 0; q < E; ++q) col[zr_out_index<T, N>(lane, q) * LD] = x[q];
+                for (int q = 0; q < E; ++q) col[pr_tile_row<T, N>(zr_out_index<T, N>(lane, q)) * LD] = x[q];
             }
             __syncthreads();   // output tile complete
             V *dst = P.out[sp.vout[fi][v]] + dbase + tid % NB;

@@ -116,15 +116,22 @@ template <typename T, int N> struct ZRCfg {
         return (SHFL || (full && TWFULL)) ? E : (E == 16 ? 4 : 3);
     }
     static constexpr int LOGE = rows(false);
-    // line padding: per 64 entries (transpose scheme, FP32 E = 8); in the
-    // shuffle scheme c entries per E, so that a warp's stores of one output
-    // element (positions q + E j, j = 0 .. 31) fall in distinct bank pairs
-    static constexpr int PADP = (sizeof(T) == 4 && E == 8) ? 8 : 0;
+    // line padding.  Transpose scheme: a warp's stores of a transform's
+    // output (zr_out_index: lane groups j = lane % G at E^2 sigma(j) apart,
+    // lanes of a group on consecutive entries) take one wavefront per 128
+    // bytes when every group starts on its own bank range, so PADP entries
+    // follow every PADB = E^2: 64 bytes for E = 16 (two groups), 32 for E = 8
+    // (four) (measured at 512^3: FP64 z 6.42 -> 6.20 ms, FP32 2.61 -> 2.53 ms;
+    // at 256^3 FP64 1.11 -> 0.96 ms).  Shuffle scheme: c entries per E, so
+    // that a warp's stores of one output element (positions q + E j,
+    // j = 0 .. 31) fall in distinct bank pairs.
+    static constexpr int PADB = SHFL ? E : E * E;
+    static constexpr int PADP = SHFL ? 0 : (E == 16 ? 64 : 32) / (int)sizeof(V2<T>);
     static constexpr int PADC = SHFL ? ((E & 1) ? 2 : 1) : 0;
     __host__ __device__ static constexpr int pidx(int n) {
-        return SHFL ? n + PADC * (n / E) : n + PADP * (n >> 6);
+        return SHFL ? n + PADC * (n / E) : n + PADP * (n / PADB);
     }
-    static constexpr int PL = SHFL ? N + PADC * 32 : N + PADP * (N / 64);   // line length in shared memory
+    static constexpr int PL = SHFL ? N + PADC * 32 : N + PADP * (N / PADB);   // line length in shared memory
     static constexpr int SCR = SHFL ? PL : E * S;       // scratch line per warp (transposes, physical line)
     static_assert(SCR >= PL, "scratch holds a padded line");
     // index into the length-N table exp(-2 pi i j / N) of twiddle-table entry i
