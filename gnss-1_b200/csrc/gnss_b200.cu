@@ -340,17 +340,21 @@ template <typename T, int N> struct Launch {
             return cudaErrorNotSupported;
         }
     }
-    // warp-specialised register z kernel (FP32, 9 quantities, 4 products)
-    static cudaError_t zws_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp, int nkz,
-                             T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm, cudaStream_t s,
-                             int nmem, long long ms) {
+    // warp-specialised register z kernel (N = 256, 512; FP32 with 9 quantities and 4 products, FP64 with 9 and 4
+    // or 12 and 5)
+    static constexpr bool zws_size() { return N == 256 || N == 512; }
+    template <int NPH, int NRAW>
+    static cudaError_t zws_kt(const FieldSet<T> &f, const ZRecipeSet &zr, int nout, long long nlines, int ncp,
+                              int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
+                              cudaStream_t s, int nmem, long long ms) {
         if (nmem > 1) return cudaErrorNotSupported;   // batches run the register z kernel
-        if constexpr ((N == 256 || N == 512) && sizeof(T) == 4) {
-            const int smem = ZRCfg<T, N>::smem_bytes_ws(ZWS_NPH, ZWS_NOUT, 10, ncp);
-            auto kern = k_zws<T, N, ZWS_NPH, 10>;
+        if constexpr (zws_size()) {
+            constexpr int NOUT = zws_nout<NPH>();
+            const int smem = ZRCfg<T, N>::smem_bytes_ws(NPH, NOUT, NRAW, ncp);
+            auto kern = k_zws<T, N, NPH, NRAW>;
             cudaError_t e = prep_smem(kern, smem);
             if (e != cudaSuccess) return e;
-            const int nt = (ZWS_NPH + ZWS_NOUT) * 32;
+            const int nt = (NPH + NOUT) * 32;
             const int per_sm = blocks_per_sm(kern, nt, smem);
             const long long mpairs = nlines / 2, npairs = mpairs * nmem;
             long long grid = (long long)per_sm * nsm;
@@ -364,12 +368,24 @@ template <typename T, int N> struct Launch {
             return cudaErrorNotSupported;
         }
     }
+    static cudaError_t zws_k(const FieldSet<T> &f, const ZRecipeSet &zr, int nph, int nraw, int nout, long long nlines,
+                             int ncp, int nkz, T scale, T alpha, double dkz, const void *tw, unsigned *err, int nsm,
+                             cudaStream_t s, int nmem, long long ms) {
+        if (nph == 9 && nraw == 10)
+            return zws_kt<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
+        if (nph == 12 && nraw == 13)
+            return zws_kt<12, 13>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
+        return cudaErrorNotSupported;
+    }
     static bool zws_fits(int nph, int nraw, int nout, int ncp) {
-        if constexpr ((N == 256 || N == 512) && sizeof(T) == 4)
-            return nph == ZWS_NPH && nraw == 10 && nout == ZWS_NOUT &&
-                   ZRCfg<T, N>::smem_bytes_ws(ZWS_NPH, ZWS_NOUT, 10, ncp) <= ZPCfg<T, N>::SMEM_MAX;
-        else
+        if constexpr (zws_size()) {
+            const bool fp32 = sizeof(T) == 4 && nph == 9 && nraw == 10 && nout == 4;
+            const bool fp64 = sizeof(T) == 8 && ((nph == 9 && nraw == 10 && nout == 4) ||
+                                                 (nph == 12 && nraw == 13 && nout == 5));
+            return (fp32 || fp64) && ZRCfg<T, N>::smem_bytes_ws(nph, nout, nraw, ncp) <= ZPCfg<T, N>::SMEM_MAX;
+        } else {
             return false;
+        }
     }
     static bool zreg_fits(int nph, int nraw, int ncp) {
         if constexpr (zr_size(N))
@@ -378,8 +394,12 @@ template <typename T, int N> struct Launch {
             return false;
     }
     // the z kernel a variant option selects: GNSS_VARIANT_WARPSPEC, _REGISTER or _STAGED
+    // AUTO: the warp-specialised kernel in FP64 where it fits (17 or 13 warps per SM against k_zreg's 12 or 9;
+    // measured at 512^3 with two scalars: z 6.18 -> 5.53 ms, one scalar 5.48 -> 4.59 ms; 256^3 0.95 -> 0.80 ms),
+    // the register kernel in FP32 (there k_zws measured slower: 2.52 -> 2.70 ms at 512^3)
     static int zkernel(int zvariant, int nph, int nraw, int nout, int ncp) {
-        if (zvariant == GNSS_VARIANT_WARPSPEC && zws_fits(nph, nraw, nout, ncp)) return GNSS_VARIANT_WARPSPEC;
+        const bool ws = zvariant == GNSS_VARIANT_WARPSPEC || (zvariant == GNSS_VARIANT_AUTO && sizeof(T) == 8);
+        if (ws && zws_fits(nph, nraw, nout, ncp)) return GNSS_VARIANT_WARPSPEC;
         const bool reg = zvariant == GNSS_VARIANT_REGISTER || zvariant == GNSS_VARIANT_WARPSPEC ||
                          (zvariant == GNSS_VARIANT_AUTO && zr_auto_z(N));
         return reg && zreg_fits(nph, nraw, ncp) ? GNSS_VARIANT_REGISTER : GNSS_VARIANT_STAGED;
@@ -402,7 +422,7 @@ template <typename T, int N> struct Launch {
         }
         const int kern = zkernel(zvariant, nph, nraw, nout, ncp);
         if (kern == GNSS_VARIANT_WARPSPEC)
-            return zws_k(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
+            return zws_k(f, zr, nph, nraw, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nmem, ms);
         if (kern == GNSS_VARIANT_REGISTER) {
             if (nph == 9 && nraw == 10)
                 return zreg_k<9, 10>(f, zr, nout, nlines, ncp, nkz, scale, alpha, dkz, tw, err, nsm, s, nullptr, nmem,

@@ -626,35 +626,37 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
 }
 
 // Warp-specialised form of k_zreg (same arguments, same results): NPH inverse
-// warps and ZWS_NOUT forward warps per block, each with its own scratch line.
+// warps and nout forward warps per block, each with its own scratch line.
 // Per line pair p, between two block barriers, the inverse warps unpack and
 // transform the quantities of p (each leaving its physical quantity in its
 // own line) while the forward warps transform and store the products of the
 // block's previous pair (held in their own lines); after the first barrier
 // the whole block forms the products of p into the forward warps' lines.
-// Every warp thus runs one length-N transform per pair instead of 4 of 9
-// warps running the forward ones alone.  The raw lines of the next pair are
-// requested as soon as every inverse warp has unpacked (named barrier 1); a
-// wait that times out sets bit 0 of *err and the block stops.  FP32 with 9
-// quantities: 13 warps, 72 registers, two blocks per SM.
-constexpr int ZWS_NPH = 9, ZWS_NOUT = 4;
+// Every warp thus runs one length-N transform per pair instead of nout of
+// NPH warps running the forward ones alone.  The raw lines of the next pair
+// are requested as soon as every inverse warp has unpacked (named barrier 1);
+// a wait that times out sets bit 0 of *err and the block stops.  FP32 with 9
+// quantities: 13 warps, 72 registers, two blocks per SM; FP64 with 9 or 12
+// quantities: 13 or 17 warps, one block per SM (k_zreg: 9 or 12).
+template <int NPH> __host__ __device__ constexpr int zws_nout() { return NPH >= 12 ? 5 : 4; }
 template <typename T, int N, int NPH, int NRAW, bool MB = false>
-__global__ void __launch_bounds__((ZWS_NPH + ZWS_NOUT) * 32, 2)
+__global__ void __launch_bounds__((NPH + zws_nout<NPH>()) * 32, sizeof(T) == 4 ? 2 : 1)
 k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet zr, int nout, long long npairs,
       int ncp, int nkz, T scale, T alpha, double dkz, const V2<T> *__restrict__ tw, unsigned *__restrict__ err,
       long long mpairs, long long ms) {
-    static_assert(NPH == ZWS_NPH && sizeof(T) == 4, "k_zws serves FP32 with 9 physical quantities");
+    constexpr int NOUT = zws_nout<NPH>();   // products (the host checks nout)
+    static_assert(NPH == 9 || NPH == 12, "k_zws serves 9 or 12 physical quantities");
     using V = V2<T>;
     using Z = ZRCfg<T, N>;
     constexpr int E = Z::E, SCR = Z::SCR;
     constexpr unsigned NINV = NPH * 32;   // threads of the inverse warps (named barrier 1)
-    (void)nout;                           // ZWS_NOUT products (the host checks)
+    (void)nout;
     const int rawf = 2 * ncp;
     const unsigned raw_bytes = (unsigned)(rawf * sizeof(V));
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
-    V *lines = tws + Z::LOGE * 32;           // NPH + ZWS_NOUT scratch lines, one per warp
-    V *raw = lines + (NPH + ZWS_NOUT) * SCR;
+    V *lines = tws + Z::LOGE * 32;           // NPH + NOUT scratch lines, one per warp
+    V *raw = lines + (NPH + NOUT) * SCR;
     uint64_t *bar = reinterpret_cast<uint64_t *>(raw + NRAW * rawf);
     T *tkz = reinterpret_cast<T *>(bar + 2);   // kz wavenumbers of the kept modes (ncp entries)
     __shared__ int stop;
@@ -685,6 +687,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
     unsigned parity = 0;
     const bool inv = warp < NPH;
     const ZRecipe rc = zr.q[inv ? warp : 0];
+    const int kind = zr_kind(rc);
     V *scr = lines + warp * SCR;
     long long prev = -1;
     for (;;) {
@@ -692,8 +695,11 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
             if (pair < npairs) {
                 const bool ok = mbar_wait_bounded(bar, parity, wc.limit);
                 V x[E];
-                zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr, ncp,
-                              keep, tkz);
+                if constexpr (sizeof(T) == 8 && E % 2 == 0)   // as k_zreg
+                    zr_pack_any<T, N>(kind, lane, x, rc, raw, rawf, ncp, nkz, keep, tkz);
+                else
+                    zr_pack<T, N>(lane, x, rc, raw + rc.r[0] * rawf, rc.r[1] >= 0 ? raw + rc.r[1] * rawf : nullptr,
+                                  ncp, keep, tkz);
                 if (bar_named_or(1, NINV, !ok)) {   // every inverse warp has unpacked, or one gave up
                     if (threadIdx.x == 0) {
                         stop = 1;

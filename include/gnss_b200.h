@@ -242,8 +242,10 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  * transforms):
  *   GNSS_VARIANT_AUTO      the kernel measured fastest on B200: register-
  *                          resident transforms where they fit (z: every N
- *                          below; x / y passes: N = 96 .. 512 in FP32,
- *                          256 and 512 in FP64), staged otherwise;
+ *                          below, with separate inverse and forward warps
+ *                          in FP64 where that kernel exists; x / y passes:
+ *                          N = 96 .. 512 in FP32, 256 and 512 in FP64),
+ *                          staged otherwise;
  *   GNSS_VARIANT_REGISTER  register-resident transforms where they exist
  *                          (N = 64, 96, 128, 192 with lane shuffles only;
  *                          N = 256, 512 with one transpose) and fit (a
@@ -251,8 +253,9 @@ gnss_status gnss_profile_read(gnss_ctx *ctx, double *ms, long long *launches);
  *   GNSS_VARIANT_STAGED    per-radix-stage transforms through shared memory;
  *   GNSS_VARIANT_WARPSPEC  (GNSS_OPT_ZVARIANT only) the register z kernel
  *                          with separate inverse and forward warps, where it
- *                          exists (FP32, one scalar, no colloid term, z
- *                          length 256 or 512); the register kernel otherwise;
+ *                          exists (z length 256 or 512, no colloid term; FP32
+ *                          with one scalar, FP64 with one or two); the
+ *                          register kernel otherwise;
  *   GNSS_VARIANT_TENSOR    (GNSS_OPT_PVARIANT only) line transforms on the
  *                          tensor cores as split-TF32 DFT-matrix GEMMs
  *                          (tcgen05, three TF32 products per GEMM with FP32

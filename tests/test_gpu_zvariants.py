@@ -132,8 +132,11 @@ def test_z_kernel_query(torch_cuda):
     cases = [
         # config, z option -> kernel
         (dict(n=256, precision=G.GNSS_FP32), W, W),
-        (dict(n=256, precision=G.GNSS_FP64), W, R),      # warp-specialised kernel: FP32 only
-        (dict(n=256, precision=G.GNSS_FP32, n_scalars=2), W, R),
+        (dict(n=256, precision=G.GNSS_FP64), W, W),      # FP64 with one or two scalars,
+        (dict(n=256, precision=G.GNSS_FP64, n_scalars=2), W, W),
+        (dict(n=256, precision=G.GNSS_FP64), A, W),      # AUTO takes it in FP64,
+        (dict(n=256, precision=G.GNSS_FP32), A, R),      # not in FP32
+        (dict(n=256, precision=G.GNSS_FP32, n_scalars=2), W, R),   # FP32 with one
         (dict(n=128, precision=G.GNSS_FP32), W, R),      # and z length 256 or 512 only
         (dict(n=128, precision=G.GNSS_FP32), A, R),
         (dict(n=128, precision=G.GNSS_FP32), S, S),
