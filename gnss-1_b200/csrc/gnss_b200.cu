@@ -52,6 +52,9 @@ struct gnss_ctx {
     //   P fields [x][kept ky][ncp], Q fields [x][y][ncp], R (in Q) [kept ky][kept kx][ncp]
     KeepMap kx_keep{}, ky_keep{};
     int nkz = 0, ncp = 0;
+    // kept Nyquist modes whose velocity the reference's transform round trip projects onto its Hermitian part
+    // (k_herm): the ky Nyquist row and the kx Nyquist column of the kz = 0 plane, the kz = nz/2 plane
+    int herm_row = 0, herm_col = 0, herm_plane = 0;
     size_t p_elems = 0, q_elems = 0;
     int zvariant = GNSS_VARIANT_AUTO;             // z kernel choice (gnss_set_option)
     int pvariant = GNSS_VARIANT_AUTO;             // x / y pass kernel choice
@@ -729,6 +732,18 @@ static gnss_status nonlinear_and_update(gnss_ctx *c, const gnss_fields *state, v
     }
     const long long nlines = (long long)g.nx * g.ny;
     const T scale = (T)(1.0 / ((double)g.nx * g.ny * g.nz));
+    if (uc.scheme == GNSS_SCHEME_CNAB2 && (c->herm_row || c->herm_col || c->herm_plane)) {
+        // the Hermitian part of the velocity at kept Nyquist modes, as the reference's round trip leaves it
+        MemberCoef mc{};
+        if (bt.nmem > 1) mc = *bt.mc;
+        else mc.mean[0] = c->mean64;
+        const long long n = ((c->herm_row ? g.nx : 0) + (c->herm_col ? g.ny : 0) +
+                             (c->herm_plane ? (long long)g.nx * g.ny : 0)) * bt.nmem;
+        k_herm<T><<<(unsigned)std::min<long long>((n + 255) / 256, 4LL * c->nsm), 256, 0, s>>>(
+            SF, g, c->herm_row, c->herm_col, c->herm_plane, mc, bt.nmem, bt.ms_sh);
+        LAUNCH_CK(c);
+        c->launches++;
+    }
     {
         StageTimer t(c, s, 0);
         PassPtrs<T> P{};
@@ -1295,6 +1310,9 @@ static void set_layout(gnss_ctx *c) {
     c->ky_keep = keep_of(g.ny, g.dky, g.kmax2);
     const KeepMap kz = keep_of(g.nz, g.dkz, g.kmax2);
     c->nkz = kz.K < 0 ? g.nz2 : kz.K + 1;
+    c->herm_row = c->ky_keep.K < 0 && g.ny % 2 == 0;
+    c->herm_col = c->kx_keep.K < 0 && g.nx % 2 == 0;
+    c->herm_plane = kz.K < 0 && g.nz % 2 == 0;
     c->ncp = (c->nkz + 15) / 16 * 16;
     c->p_elems = (size_t)g.nx * c->ky_keep.count() * c->ncp;
     c->q_elems = (size_t)g.nx * g.ny * c->ncp;

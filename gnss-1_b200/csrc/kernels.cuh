@@ -906,6 +906,57 @@ template <typename T> __global__ void k_dealias(V2<T> *f, Geom g) {
     }
 }
 
+// The reference's solver_ps takes the velocity through an inverse and a
+// forward transform before the vorticity and the time step use it
+// (solver.cu:707-722, :743-750).  The complex-to-real z transform of that
+// round trip keeps the Hermitian part of the kz = 0 and kz = nz/2 planes,
+// F(k) -> (F(k) + conj F(-k)) / 2.  The velocity of a state departs from
+// that symmetry only at kept Nyquist modes: makeRHS (solver.cu:461-521)
+// projects a Nyquist mode and its mirror with the same wavenumber -n/2, so
+// the projected right-hand side there is not Hermitian.  k_herm applies the
+// round trip's projection to u, v, w where that can happen:
+//   in the kz = 0 plane, the ky Nyquist row (row_y) and the kx Nyquist
+//   column (col_x), mirror (-kx, -ky);
+//   the whole kz = nz/2 plane (plane_z), mirror (-kx, -ky).
+// One thread per pair of mirror modes (a mode that is its own mirror keeps
+// its real part).  In FP32 contexts the FP64 mean-profile entry of the ky
+// Nyquist row (mc.mean[member]) gets the same treatment.  Members of a batch
+// are ms elements apart.
+template <typename T>
+__global__ void k_herm(FieldSet<T> f, Geom g, int row_y, int col_x, int plane_z, const __grid_constant__ MemberCoef mc,
+                       int nmem, long long ms) {
+    using V = V2<T>;
+    const int nx = g.nx, ny = g.ny;
+    const long long na = row_y ? nx : 0, nb = col_x ? ny : 0, nc = plane_z ? (long long)nx * ny : 0;
+    const long long per = na + nb + nc;
+    GNSS_GRID_STRIDE(per * nmem) {
+        const int mi = (int)(idx / per);
+        long long t = idx - (long long)mi * per;
+        int i, j, kz;
+        if (t < na) {   // kz = 0, ky Nyquist row
+            i = (int)t; j = ny / 2; kz = 0;
+        } else if ((t -= na) < nb) {   // kz = 0, kx Nyquist column (its ky Nyquist entry belongs to the row)
+            i = nx / 2; j = (int)t; kz = 0;
+            if (row_y && j == ny / 2) continue;
+        } else {   // kz = nz/2 plane
+            t -= nb;
+            j = (int)(t / nx); i = (int)(t - (long long)j * nx); kz = g.nz / 2;
+        }
+        const int mi2 = (nx - i) % nx, mj2 = (ny - j) % ny;
+        if ((long long)mj2 * nx + mi2 < (long long)j * nx + i) continue;   // the pair is done from its other mode
+        const long long a = ((long long)j * nx + i) * g.nz2 + kz + (long long)mi * ms;
+        const long long b = ((long long)mj2 * nx + mi2) * g.nz2 + kz + (long long)mi * ms;
+        double2 *const mean = mc.mean[mi];
+        for (int q = 0; q < 3; ++q) {
+            const V x = f.p[q][a], y = f.p[q][b];
+            const V h = V{T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y)};
+            f.p[q][a] = h;
+            f.p[q][b] = V{h.x, -h.y};
+            if (mean && kz == 0 && i == 0 && a == b) mean[q * ny + j].y = 0.0;   // the FP64 mean-profile entry
+        }
+    }
+}
+
 template <typename T>
 __global__ void k_vorticity(const V2<T> *u, const V2<T> *v, const V2<T> *w, V2<T> *o1, V2<T> *o2, V2<T> *o3, Geom g) {
     using V = V2<T>;

@@ -29,7 +29,7 @@ if [ ! -f "$REF/solver.cu" ]; then
     exit 1
 fi
 
-# name  N    Re      Sc   Sc_c  alpha  dt      pert_amp (noise of the initial jet, initialize.cu:615-641)
+# name  N (or NXxNYxNZ)  Re  Sc  Sc_c  alpha  dt  pert_amp (noise of the initial jet, initialize.cu:615-641)
 CONFIGS="
 g12    12   200.0   0.7  1.0   0.0    2.0e-3  0.0
 g16    16   200.0   0.7  1.0   0.0    2.0e-3  0.0
@@ -40,21 +40,26 @@ c64    64   1000.0  0.7  0.7   0.0    1.0e-3  0.0
 c128   128  1000.0  0.7  0.7   0.0    1.0e-3  0.0
 c256   256  3000.0  0.7  1.0   0.0    5.0e-4  0.0
 c512   512  5000.0  0.7  0.7   0.0    2.5e-4  0.0
+n64y32 64x32x64 800.0 0.7 1.0  0.0    1.0e-3  0.0
 "
 
 want=("$@")
 SRCS=(solver cudafuncs fftfuncs allocate initialize iofuncs statistics)
 
-gen_params() {  # N Re Sc Sc_c alpha dt pert_amp
+gen_params() {  # N-or-NXxNYxNZ Re Sc Sc_c alpha dt pert_amp
+    local nx ny nz
+    IFS=x read -r nx ny nz <<< "$1"
+    ny=${ny:-$nx}
+    nz=${nz:-$nx}
     cat <<EOF
 /* generated by oracle/build_ref.sh: the temporal-jet configuration of the
  * reference (dnsparams.h:9-41) with runtime sizes fixed for this build */
 #define TX 8
 #define TY 8
 #define TZ 8
-#define NX $1
-#define NY $1
-#define NZ $1
+#define NX $nx
+#define NY $ny
+#define NZ $nz
 #define NZ2 (NZ/2 + 1)
 #define NN (NX*NY*NZ)
 #define PI (M_PI)

@@ -103,6 +103,45 @@ def test_live_reference_256_two_scalars(torch_cuda):
 
 
 @pytest.mark.gpu
+def test_live_reference_kept_nyquist_row(torch_cuda, oracle):
+    """The reference program on a 64 x 32 x 64 grid (Re 800, Sc 0.7 / 1.0, dt 1e-3): its dealiasing radius
+    alias_filter * NX / 2 (solver.cu:29-31) keeps the ky Nyquist row, where the velocity's round trip through
+    physical space (solver.cu:707-722, :743-750) leaves only the Hermitian part of the kz = 0 plane.  This
+    library and the oracle both match the reference's states after each of 4 steps."""
+    import gnss_b200 as G
+    torch = torch_cuda
+    exe = _refdrv("n64y32")
+    nx, ny, nz, steps = 64, 32, 64, 4
+    f = G.jet_initial_state(nx, ny, nz, n_scalars=2, seed=1, noise_kmax=6.0, amp=0.05)
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        with open(td / "ic.bin", "wb") as fp:
+            for a in f:
+                fp.write(np.ascontiguousarray(a).tobytes())
+        r = subprocess.run([str(exe), "run", str(td / "ic.bin"), str(steps), str(td), "1,2,3,4"],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        ref = [np.fromfile(td / f"state_{s}.bin", dtype=np.complex128).reshape(5, ny, nx, nz // 2 + 1)
+               for s in range(1, steps + 1)]
+    oc = oracle.cfg(nx=nx, ny=ny, nz=nz, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3)
+    o = [a.copy() for a in f]
+    ro = [np.zeros_like(f[0]) for _ in range(5)]
+    with G.Context(nx=nx, ny=ny, nz=nz, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3, n_scalars=2) as ctx:
+        st = [to_dev(torch, a) for a in f]
+        hi = [torch.zeros_like(st[0]) for _ in st]
+        ctx.de_alias(st)
+        for s in range(steps):
+            ctx.solver_ps(st, hi, euler=(s == 0))
+            oracle.step_cnab2(oc, o, ro, euler=(s == 0))
+            tol = 1e-12 if s == 0 else 1e-11
+            for q in range(5):
+                e_lib = rel_l2(to_host(st[q]), ref[s][q])
+                e_orc = rel_l2(o[q], ref[s][q])
+                assert e_lib < tol, (s + 1, q, "library", e_lib)
+                assert e_orc < tol, (s + 1, q, "oracle", e_orc)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("cfg,n,ns,steps", [("g16a", 16, 2, 4), ("c64", 64, 1, 5)])
 def test_dropin_shim_matches_reference_program(torch_cuda, cfg, n, ns, steps):
     """The same driver linked two ways: the reference's solver.o + fftfuncs.o
