@@ -30,6 +30,7 @@ if [ ! -f "$REF/solver.cu" ]; then
 fi
 
 # name  N (or NXxNYxNZ)  Re  Sc  Sc_c  alpha  dt  pert_amp (noise of the initial jet, initialize.cu:615-641)
+#       [alias_filter (default 2/3; 15/16 is the reference's 15/32 rule, dnsparams.h:91)] [L in units of pi (default 2)]
 CONFIGS="
 g12    12   200.0   0.7  1.0   0.0    2.0e-3  0.0
 g16    16   200.0   0.7  1.0   0.0    2.0e-3  0.0
@@ -41,13 +42,16 @@ c128   128  1000.0  0.7  0.7   0.0    1.0e-3  0.0
 c256   256  3000.0  0.7  1.0   0.0    5.0e-4  0.0
 c512   512  5000.0  0.7  0.7   0.0    2.5e-4  0.0
 n64y32 64x32x64 800.0 0.7 1.0  0.0    1.0e-3  0.0
+a64    64   800.0   0.7  1.0   0.0    1.0e-3  0.0     (15.0/16.0)
+l64    64   800.0   0.7  1.0   0.0    1.0e-3  0.0     (2.0/3.0)  4.0
 "
 
 want=("$@")
 SRCS=(solver cudafuncs fftfuncs allocate initialize iofuncs statistics)
 
-gen_params() {  # N-or-NXxNYxNZ Re Sc Sc_c alpha dt pert_amp
+gen_params() {  # N-or-NXxNYxNZ Re Sc Sc_c alpha dt pert_amp [alias_filter] [L/pi]
     local nx ny nz
+    local af=${8:-"(2.0/3.0)"} lpi=${9:-2.0}
     IFS=x read -r nx ny nz <<< "$1"
     ny=${ny:-$nx}
     nz=${nz:-$nx}
@@ -63,9 +67,9 @@ gen_params() {  # N-or-NXxNYxNZ Re Sc Sc_c alpha dt pert_amp
 #define NZ2 (NZ/2 + 1)
 #define NN (NX*NY*NZ)
 #define PI (M_PI)
-#define LX (2.0*PI)
-#define LY (2.0*PI)
-#define LZ (2.0*PI)
+#define LX ($lpi*PI)
+#define LY ($lpi*PI)
+#define LZ ($lpi*PI)
 #define DX (LX/NX)
 #define n_checkpoint 1000000
 #define n_vis 1000000
@@ -81,7 +85,7 @@ gen_params() {  # N-or-NXxNYxNZ Re Sc Sc_c alpha dt pert_amp
 #define Sc $3
 #define Sc_c $4
 #define alpha $5
-#define alias_filter (2.0/3.0)
+#define alias_filter $af
 #define pert_amp $7
 #define rootdir "./"
 #define sim_name "refdrv/"
@@ -90,7 +94,7 @@ EOF
 }
 
 build_one() {
-    local name=$1 n=$2 re=$3 sc=$4 scc=$5 al=$6 dtv=$7 pert=$8
+    local name=$1 n=$2 re=$3 sc=$4 scc=$5 al=$6 dtv=$7 pert=$8 af=${9:-} lpi=${10:-}
     local d="$OUT/$name"
     mkdir -p "$d/src" "$d/obj"
     for f in "$REF"/*.cu "$REF"/*.h; do
@@ -98,7 +102,7 @@ build_one() {
         [ "$b" = "dnsparams.h" ] && continue
         ln -sf "$f" "$d/src/$b"
     done
-    gen_params "$n" "$re" "$sc" "$scc" "$al" "$dtv" "$pert" > "$d/src/dnsparams.h"
+    gen_params "$n" "$re" "$sc" "$scc" "$al" "$dtv" "$pert" $af $lpi > "$d/src/dnsparams.h"
     local objs=()
     for s in "${SRCS[@]}"; do
         # the reference is C++03 code (Makefile:2); C99 "complex double" needs it
@@ -125,14 +129,14 @@ build_one() {
 }
 
 pids=()
-while read -r name n re sc scc al dtv pert; do
+while read -r name n re sc scc al dtv pert af lpi; do
     [ -z "${name:-}" ] && continue
     if [ ${#want[@]} -gt 0 ]; then
         keep=0
         for w in "${want[@]}"; do [ "$w" = "$name" ] && keep=1; done
         [ $keep -eq 0 ] && continue
     fi
-    build_one "$name" "$n" "$re" "$sc" "$scc" "$al" "$dtv" "$pert" &
+    build_one "$name" "$n" "$re" "$sc" "$scc" "$al" "$dtv" "$pert" $af $lpi &
     pids+=($!)
 done <<< "$CONFIGS"
 rc=0

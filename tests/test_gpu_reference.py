@@ -102,17 +102,31 @@ def test_live_reference_256_two_scalars(torch_cuda):
     print(f"worst statistic deviation over {steps} steps: {worst:.2e}")
 
 
+# Reference builds of configurations beside the cubic 2/3-rule jets (oracle/build_ref.sh):
+#   n64y32  64 x 32 x 64: the dealiasing radius alias_filter * NX / 2 (solver.cu:29-31) keeps the ky Nyquist row,
+#           where the velocity's round trip through physical space (solver.cu:707-722, :743-750) leaves only the
+#           Hermitian part of the kz = 0 plane;
+#   a64     64^3 with the reference's 15/32 truncation (dnsparams.h:91; alias_filter 15/16): kept boxes of 61 of 64
+#           rows and 31 of 33 kz modes;
+#   l64     64^3 in a (4 pi)^3 box: wavenumbers 2 pi / L = 1/2 (initialize.cu:686-689) and the radius scaled with them.
+LIVE_CONFIGS = [("n64y32", (64, 32, 64), 2.0 / 3.0, 2.0), ("a64", (64, 64, 64), 15.0 / 16.0, 2.0),
+                ("l64", (64, 64, 64), 2.0 / 3.0, 4.0)]
+
+
 @pytest.mark.gpu
-def test_live_reference_kept_nyquist_row(torch_cuda, oracle):
-    """The reference program on a 64 x 32 x 64 grid (Re 800, Sc 0.7 / 1.0, dt 1e-3): its dealiasing radius
-    alias_filter * NX / 2 (solver.cu:29-31) keeps the ky Nyquist row, where the velocity's round trip through
-    physical space (solver.cu:707-722, :743-750) leaves only the Hermitian part of the kz = 0 plane.  This
-    library and the oracle both match the reference's states after each of 4 steps."""
+@pytest.mark.parametrize("cfg,shape,alias,lpi", LIVE_CONFIGS, ids=[c[0] for c in LIVE_CONFIGS])
+def test_live_reference_configs(torch_cuda, oracle, cfg, shape, alias, lpi):
+    """The reference program, Re 800, Sc 0.7 / 1.0, dt 1e-3, two scalars: this library and the oracle both match its
+    states after each of 4 steps (1e-12 after the first, 1e-11 after the others)."""
     import gnss_b200 as G
     torch = torch_cuda
-    exe = _refdrv("n64y32")
-    nx, ny, nz, steps = 64, 32, 64, 4
-    f = G.jet_initial_state(nx, ny, nz, n_scalars=2, seed=1, noise_kmax=6.0, amp=0.05)
+    exe = _refdrv(cfg)
+    nx, ny, nz = shape
+    steps = 4
+    L = lpi * np.pi
+    kw = dict(lx=L, ly=L, lz=L, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3, alias_filter=alias)
+    f = G.jet_initial_state(nx, ny, nz, lx=L, ly=L, lz=L, n_scalars=2, seed=1, noise_kmax=6.0 * 2.0 / lpi,
+                            amp=0.05)
     with tempfile.TemporaryDirectory() as td:
         td = Path(td)
         with open(td / "ic.bin", "wb") as fp:
@@ -123,10 +137,10 @@ def test_live_reference_kept_nyquist_row(torch_cuda, oracle):
         assert r.returncode == 0, r.stderr[-2000:]
         ref = [np.fromfile(td / f"state_{s}.bin", dtype=np.complex128).reshape(5, ny, nx, nz // 2 + 1)
                for s in range(1, steps + 1)]
-    oc = oracle.cfg(nx=nx, ny=ny, nz=nz, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3)
+    oc = oracle.cfg(nx=nx, ny=ny, nz=nz, **kw)
     o = [a.copy() for a in f]
     ro = [np.zeros_like(f[0]) for _ in range(5)]
-    with G.Context(nx=nx, ny=ny, nz=nz, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3, n_scalars=2) as ctx:
+    with G.Context(nx=nx, ny=ny, nz=nz, n_scalars=2, **kw) as ctx:
         st = [to_dev(torch, a) for a in f]
         hi = [torch.zeros_like(st[0]) for _ in st]
         ctx.de_alias(st)
