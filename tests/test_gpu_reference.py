@@ -108,14 +108,18 @@ def test_live_reference_256_two_scalars(torch_cuda):
 #           Hermitian part of the kz = 0 plane;
 #   a64     64^3 with the reference's 15/32 truncation (dnsparams.h:91; alias_filter 15/16): kept boxes of 61 of 64
 #           rows and 31 of 33 kz modes;
-#   l64     64^3 in a (4 pi)^3 box: wavenumbers 2 pi / L = 1/2 (initialize.cu:686-689) and the radius scaled with them.
-LIVE_CONFIGS = [("n64y32", (64, 32, 64), 2.0 / 3.0, 2.0), ("a64", (64, 64, 64), 15.0 / 16.0, 2.0),
-                ("l64", (64, 64, 64), 2.0 / 3.0, 4.0)]
+#   l64     64^3 in a (4 pi)^3 box: wavenumbers 2 pi / L = 1/2 (initialize.cu:686-689) and the radius scaled with them;
+#   r96a    96^3 (radix 3: the lane-shuffle register kernels) with the colloid term alpha = 0.05 (14 physical
+#           quantities in the z kernel);
+#   m48     48 x 96 x 64 (mixed radix, nx < ny).
+LIVE_CONFIGS = [("n64y32", (64, 32, 64), 2.0 / 3.0, 2.0, 0.0), ("a64", (64, 64, 64), 15.0 / 16.0, 2.0, 0.0),
+                ("l64", (64, 64, 64), 2.0 / 3.0, 4.0, 0.0), ("r96a", (96, 96, 96), 2.0 / 3.0, 2.0, 0.05),
+                ("m48", (48, 96, 64), 2.0 / 3.0, 2.0, 0.0)]
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cfg,shape,alias,lpi", LIVE_CONFIGS, ids=[c[0] for c in LIVE_CONFIGS])
-def test_live_reference_configs(torch_cuda, oracle, cfg, shape, alias, lpi):
+@pytest.mark.parametrize("cfg,shape,alias,lpi,alpha", LIVE_CONFIGS, ids=[c[0] for c in LIVE_CONFIGS])
+def test_live_reference_configs(torch_cuda, oracle, cfg, shape, alias, lpi, alpha):
     """The reference program, Re 800, Sc 0.7 / 1.0, dt 1e-3, two scalars: this library and the oracle both match its
     states after each of 4 steps (1e-12 after the first, 1e-11 after the others)."""
     import gnss_b200 as G
@@ -124,7 +128,7 @@ def test_live_reference_configs(torch_cuda, oracle, cfg, shape, alias, lpi):
     nx, ny, nz = shape
     steps = 4
     L = lpi * np.pi
-    kw = dict(lx=L, ly=L, lz=L, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3, alias_filter=alias)
+    kw = dict(lx=L, ly=L, lz=L, re=800.0, sc=0.7, sc_c=1.0, dt=1e-3, alias_filter=alias, alpha=alpha)
     f = G.jet_initial_state(nx, ny, nz, lx=L, ly=L, lz=L, n_scalars=2, seed=1, noise_kmax=6.0 * 2.0 / lpi,
                             amp=0.05)
     with tempfile.TemporaryDirectory() as td:
