@@ -88,6 +88,22 @@ __device__ __forceinline__ bool bar_named_or(unsigned id, unsigned nthreads, boo
     return r != 0;
 }
 
+// ------------------------------------------------- programmatic dependent launch
+// A step kernel launched with programmatic stream serialization may start
+// (its prologue: twiddle tables, shared-memory barriers) on SMs the previous
+// kernel in the stream has left.  pdl_wait() blocks until that kernel has
+// completed and its memory is visible; a kernel calls it before its first
+// access to global memory another step kernel writes or reads.
+// pdl_trigger() lets the next kernel launch once every block of this one has
+// called it or exited.  The short kernels (update, Hermitian projection,
+// statistics) call it at their start; the persistent ones do not, and their
+// blocks trigger by exiting (a trigger tested inside their main loops cost
+// the 512^3 FP64 step 1%).  Without that launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// (no memory clobber: the trigger only lets the next grid be scheduled; its
+// pdl_wait, not the trigger, orders the memory)
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 // ---------------------------------------------------------------- cp.async
 // Per-thread asynchronous copies global -> shared (LDGSTS).  src_bytes = 0
 // fills the destination with zeros without reading the source.

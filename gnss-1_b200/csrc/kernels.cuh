@@ -169,6 +169,7 @@ k_pass(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec s
         const V *src = P.in[fi] + (MB ? mi * sp.ms_in : 0LL) + (long long)(sp.outer_in_compact ? oc : o) * sp.s_out + c0;
         tile_prefetch<T, NB, NT, TILE>(dst, src, sp, c0, tid);
     };
+    pdl_wait();
     prefetch(item, rawb[0]);
     cp_async_commit();
     int buf = 0;
@@ -519,6 +520,7 @@ k_zphys(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSe
         }
         __syncthreads();
     }
+    pdl_wait();
     const WaitCtl wc(err);
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
@@ -648,6 +650,8 @@ __device__ __forceinline__ void k_update_body(const FieldSet<T> &state, const Fi
                                               double2 *__restrict__ mean0, const MemberCoef *mc, int nmem,
                                               long long ms_sh, long long ms_nl) {
     using V = V2<T>;
+    pdl_wait();
+    pdl_trigger();
     double acc[STATS ? STAT_SUMS : 1] = {};
     const int nkx = kx_keep.count(), nky = ky_keep.count();
     const int mrows = nky * nkx;   // rows of one member
@@ -884,6 +888,8 @@ k_stats_partial(FieldSet<T> st, int has_s, int has_c, Geom g, double *__restrict
 __global__ void __launch_bounds__(STAT_SUMS * 32) k_stats_final(const double *__restrict__ partial, int nblocks,
                                                                  double *__restrict__ out) {
     // warp q sums column q: lanes stride the blocks, then a fixed shuffle tree
+    pdl_wait();
+    pdl_trigger();
     const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Kahan acc;
     for (int b = lane; b < nblocks; b += 32) acc.add(partial[b * STAT_SUMS + q]);
@@ -926,6 +932,8 @@ template <typename T>
 __global__ void k_herm(FieldSet<T> f, Geom g, int row_y, int col_x, int plane_z, const __grid_constant__ MemberCoef mc,
                        int nmem, long long ms) {
     using V = V2<T>;
+    pdl_wait();
+    pdl_trigger();
     const int nx = g.nx, ny = g.ny;
     const long long na = row_y ? nx : 0, nb = col_x ? ny : 0, nc = plane_z ? (long long)nx * ny : 0;
     const long long per = na + nb + nc;

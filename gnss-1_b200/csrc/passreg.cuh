@@ -131,6 +131,7 @@ k_passr(const __grid_constant__ PassPtrs<T> P, const __grid_constant__ PassSpec 
             else cp_async8(dst + row * LD + b, p, 8);
         }
     };
+    pdl_wait();
     prefetch(item, tiles);
     cp_async_commit();
     int buf = 0;

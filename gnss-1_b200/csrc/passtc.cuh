@@ -94,6 +94,8 @@ k_passtc(const __grid_constant__ PassPtrs<float> P, const __grid_constant__ Pass
     using C = PTCfg<N>;
     using V = float2;
     constexpr int NB = C::NB, N1 = C::N1, N2 = C::N2, NIT = C::NIT, KQ = C::KQ;
+    pdl_wait();   // before the prologue too: its TMEM allocation waits for the previous kernel's blocks
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
     const uint32_t base = (raw_addr + 1023u) & ~1023u;

@@ -564,6 +564,7 @@ k_zreg(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet
         mbar_fence_init();
     }
     __syncthreads();
+    pdl_wait();
     const WaitCtl wc(err);
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
@@ -677,6 +678,7 @@ k_zws(const __grid_constant__ FieldSet<T> f, const __grid_constant__ ZRecipeSet 
         mbar_fence_init();
     }
     __syncthreads();
+    pdl_wait();
     const WaitCtl wc(err);
     auto issue = [&](long long p, bool withhold = false) {
         mbar_arrive_expect_tx(bar, NRAW * raw_bytes);
