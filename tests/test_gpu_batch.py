@@ -102,6 +102,34 @@ def test_ensemble_batched_groups_match_alone(torch_cuda):
 
 
 @pytest.mark.gpu
+def test_ensemble_batched_kept_nyquist_row(torch_cuda):
+    """Groups whose dealiasing radius keeps the ky Nyquist row (96 x 64 x 96: alias_filter * 96 / 2 = 32 = ny / 2),
+    where the velocity there is projected onto its Hermitian part at the start of each step, as the reference's round
+    trip through physical space leaves it: 2 FP64 and 2 FP32 members, batched, end bit-identical to the same jets
+    run alone."""
+    import gnss_b200 as G
+    cfgs = [G.make_config(nx=96, ny=64, nz=96, re=re, sc=0.7, sc_c=1.0, dt=1e-3, n_scalars=2, precision=p)
+            for p in (G.GNSS_FP64, G.GNSS_FP32) for re in (600.0, 1300.0)]
+    init = [_init(G, c, seed=40 + i) for i, c in enumerate(cfgs)]
+    with G.Ensemble(cfgs, n_branches=2) as ens:
+        ens.set_batching(True)
+        assert all(ens.batched(i) for i in range(len(cfgs)))
+        for i, a in enumerate(init):
+            ens.upload(i, a)
+        ens.step(1)
+        ens.step(4)
+        ens.step(4)
+        got = []
+        for i, a in enumerate(init):
+            out = np.empty_like(a)
+            ens.download(i, out)
+            got.append(out)
+    for i, (c, a) in enumerate(zip(cfgs, init)):
+        ref, _ = _alone(G, c, a, 9)
+        assert np.array_equal(got[i], ref), f"member {i} differs from the jet run alone"
+
+
+@pytest.mark.gpu
 def test_ensemble_autotune_keeps_results(torch_cuda):
     import gnss_b200 as G
     cfgs = [G.make_config(256, re=2000.0, dt=5e-4, precision=G.GNSS_FP32),
