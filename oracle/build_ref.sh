@@ -46,6 +46,7 @@ a64    64   800.0   0.7  1.0   0.0    1.0e-3  0.0     (15.0/16.0)
 l64    64   800.0   0.7  1.0   0.0    1.0e-3  0.0     (2.0/3.0)  4.0
 r96a   96   800.0   0.7  1.0   0.05   1.0e-3  0.0
 m48    48x96x64 800.0 0.7 1.0  0.0    1.0e-3  0.0
+f48    48   800.0   0.7  1.0   0.0    1.0e-3  0.0     (1.0)
 "
 
 want=("$@")

@@ -111,10 +111,12 @@ def test_live_reference_256_two_scalars(torch_cuda):
 #   l64     64^3 in a (4 pi)^3 box: wavenumbers 2 pi / L = 1/2 (initialize.cu:686-689) and the radius scaled with them;
 #   r96a    96^3 (radix 3: the lane-shuffle register kernels) with the colloid term alpha = 0.05 (14 physical
 #           quantities in the z kernel);
-#   m48     48 x 96 x 64 (mixed radix, nx < ny).
+#   m48     48 x 96 x 64 (mixed radix, nx < ny);
+#   f48     48^3 with alias_filter 1 (no truncation): every Nyquist row, column and plane is kept, so the Hermitian
+#           projection of the velocity acts on the kx and ky Nyquist lines of the kz = 0 plane and on the kz = 24 plane.
 LIVE_CONFIGS = [("n64y32", (64, 32, 64), 2.0 / 3.0, 2.0, 0.0), ("a64", (64, 64, 64), 15.0 / 16.0, 2.0, 0.0),
                 ("l64", (64, 64, 64), 2.0 / 3.0, 4.0, 0.0), ("r96a", (96, 96, 96), 2.0 / 3.0, 2.0, 0.05),
-                ("m48", (48, 96, 64), 2.0 / 3.0, 2.0, 0.0)]
+                ("m48", (48, 96, 64), 2.0 / 3.0, 2.0, 0.0), ("f48", (48, 48, 48), 1.0, 2.0, 0.0)]
 
 
 @pytest.mark.gpu
